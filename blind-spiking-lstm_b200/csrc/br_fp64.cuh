@@ -1,0 +1,380 @@
+// Batched blind rotation (collapsed CMux chain) in FP64, K ciphertexts per CTA.
+//
+// Semantics follow the reference's JAX statement of the kernel
+// (schemas/text_jax.py:390-435, cuTFHE/multiply.py:54-92): for each group g
+//   dec   = decomposition(ACC)                    (polynomial_jax.py:90-111)
+//   ACC'  = cmod_q(round(iFFT( sum_bc DEC_F[bc] * sum_m ROT[r_gm] BSK[g,a,bc,m] )))
+// with the group's rotation indices r = round(2N <a_g,p> / (q n_lut)) n_lut
+// mod 2N (multiply.py:70-79).  Decomposition, rounding and the centred
+// reduction are the reference's float64 operations, so every stage but the
+// FFT rounding is bit-identical; with |FFT error| < 1/2 the products are too.
+//
+// Work mapping (NT = 2 K H/8 threads):
+//  * each thread owns one radix-8 butterfly (k, a, n1) of the first forward /
+//    last inverse superstage and keeps ACC[k][a][n1 + (H/8) n2] and
+//    ACC[k][a][n1 + (H/8) n2 + H] (n2 < 8) in registers across groups;
+//  * middle superstages run over all polynomials in shared memory;
+//  * the pointwise stage maps lanes to (slot p, ciphertext k) with k fastest,
+//    so the K lanes of one slot load the same key word in one request.
+#pragma once
+
+#include "tfhe_internal.cuh"
+
+namespace tfhe {
+
+struct BrArgs {
+    const double2* bsk;       // native [G][2][P][M][H]; reference layout (G,2,L,2,M,H)
+    const double2* all_rot;   // reference layout only: (2N, H)
+    const double2* qt;
+    const double2* tw;
+    const uint16_t* freq;
+    int G, M, collapse, K;
+    long long B;
+    int log2_beta, log2_q;
+    // native inputs (u32 torus)
+    const uint32_t* lwe_a;    // (B, lwe_n) key-switched masks
+    const uint32_t* lwe_b;    // (B)
+    const uint32_t* lut;      // (B|1, 2, N)
+    long long lut_stride;     // 0 or 2N
+    int n_lut, lwe_n;
+    // reference-layout inputs (mul_bootstrap drop-in)
+    const int64_t* ct_init;   // (B|1, 2, N)
+    long long ct_stride;      // 0 or 2N
+    const int32_t* indices;   // (B, G, M)
+    // outputs
+    uint32_t* acc_out;        // (B, 2, N): ACC rotated by -b~ (BR)
+    uint32_t* out_a;          // (B, n_lut, N): extracted masks
+    uint32_t* out_b;          // (B, n_lut)
+    int64_t* out_i64;         // (B, 2, N): reference-layout result
+};
+
+// coefficient of X^e (any integer e) of a negacyclic polynomial in smem
+template <int LOGN>
+__device__ __forceinline__ uint32_t ncoef(const uint32_t* p, int e) {
+    constexpr int N = 1 << LOGN;
+    e &= (2 * N - 1);
+    const uint32_t v = p[e & (N - 1)];
+    return (e < N) ? v : (0u - v);
+}
+
+// inverse superstages s = S0 .. 1 (descending) over the 2K output polys
+template <int LOGH, int s>
+__device__ __forceinline__ void inverse_middle(double2* dec, int K, int P, const double2* tw, int tid, int nt) {
+    if constexpr (s >= 1) {
+        using PL = Plan<LOGH>;
+        constexpr int R = PL::radix(s);
+        constexpr int S = PL::span(s);
+        constexpr int PER = PL::H / R;
+        const double2* tws = tw + PL::tw_offset(s);
+        const int total = 2 * K * PER;
+        for (int t = tid; t < total; t += nt) {
+            const int poly = t / PER;
+            double2* base = dec + (size_t)(poly >> 1) * P * PL::H + (poly & 1) * PL::H;
+            dit_stage<R, S>(base, tws, t % PER);
+        }
+        __syncthreads();
+        inverse_middle<LOGH, s - 1>(dec, K, P, tw, tid, nt);
+    }
+}
+
+template <int LOGH, int s>
+__device__ __forceinline__ void forward_middle(double2* dec, int npoly, const double2* tw, int tid, int nt) {
+    using PL = Plan<LOGH>;
+    if constexpr (s < PL::NS) {
+        stage_all<LOGH, s, false>(dec, npoly, tw, tid, nt);
+        __syncthreads();
+        forward_middle<LOGH, s + 1>(dec, npoly, tw, tid, nt);
+    }
+}
+
+template <int LOGN, int L, bool REFLAYOUT>
+__global__ void __launch_bounds__(512, 1) br_fp64_kernel(const BrArgs args) {
+    constexpr int N = 1 << LOGN;
+    constexpr int H = N / 2;
+    constexpr int LOGH = LOGN - 1;
+    constexpr int P = 2 * L;
+    constexpr int Q8 = H / 8;
+    using PL = Plan<LOGH>;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = args.K;
+    const int M = args.M;
+    double2* dec = reinterpret_cast<double2*>(smem_raw);           // K * P * H
+    double2* qt = dec + (size_t)K * P * H;                          // N / 2
+    double2* tw = qt + N / 2;                                       // PL::TW
+    uint16_t* freq = reinterpret_cast<uint16_t*>(tw + PL::TW);      // H
+    int* rot = reinterpret_cast<int*>(freq + H);                    // K * M
+    int* bexp = rot + K * M;                                        // K
+
+    const int tid = threadIdx.x;
+    const int nt = blockDim.x;
+    const long long ct0 = (long long)blockIdx.x * K;
+
+    for (int i = tid; i < N / 2; i += nt) qt[i] = args.qt[i];
+    for (int i = tid; i < PL::TW; i += nt) tw[i] = args.tw[i];
+    for (int i = tid; i < H; i += nt) freq[i] = args.freq[i];
+
+    // the butterfly this thread owns in the first / last superstage
+    const int ok = tid / (2 * Q8);
+    const int oa = (tid / Q8) & 1;
+    const int on1 = tid % Q8;
+    const long long oct = min(ct0 + ok, args.B - 1);
+
+    const double q = ldexp(1.0, args.log2_q);
+    const double inv_q = ldexp(1.0, -args.log2_q);
+    const double beta = ldexp(1.0, args.log2_beta);
+    constexpr double inv_h = 1.0 / H;
+
+    double acc_lo[8], acc_hi[8];
+    if constexpr (REFLAYOUT) {
+        const int64_t* src = args.ct_init + oct * args.ct_stride + oa * N;
+#pragma unroll
+        for (int n2 = 0; n2 < 8; ++n2) {
+            acc_lo[n2] = (double)src[on1 + Q8 * n2];
+            acc_hi[n2] = (double)src[on1 + Q8 * n2 + H];
+        }
+    } else {
+        const uint32_t* src = args.lut + oct * args.lut_stride + oa * N;
+#pragma unroll
+        for (int n2 = 0; n2 < 8; ++n2) {
+            acc_lo[n2] = (double)(int32_t)src[on1 + Q8 * n2];
+            acc_hi[n2] = (double)(int32_t)src[on1 + Q8 * n2 + H];
+        }
+    }
+    __syncthreads();
+
+    for (int g = 0; g < args.G; ++g) {
+        // rotation index of every (ciphertext, pattern) of this group
+        for (int t = tid; t < K * M; t += nt) {
+            const int k = t / M;
+            const int m = t - k * M;
+            const long long ct = min(ct0 + k, args.B - 1);
+            int r;
+            if constexpr (REFLAYOUT) {
+                r = args.indices[(ct * args.G + g) * M + m];
+            } else {
+                // <a_g, pattern m>, patterns in meshgrid 'ij' order
+                double v = 0.0;
+                const uint32_t* a = args.lwe_a + ct * args.lwe_n + (long long)g * args.collapse;
+                for (int c = 0; c < args.collapse; ++c)
+                    if ((m >> (args.collapse - 1 - c)) & 1) v += (double)(int32_t)a[c];
+                const double idx = rint((2.0 * N * v) / (q * args.n_lut)) * args.n_lut;
+                int ri = (int)idx % (2 * N);
+                r = ri < 0 ? ri + 2 * N : ri;
+            }
+            rot[t] = r;
+        }
+
+        // prologue: gadget digits of the owned coefficients (float64 steps of
+        // polynomial_jax.py:98-111), fold + twist, first DIF superstage
+        {
+            double x_lo[8], x_hi[8];
+#pragma unroll
+            for (int n2 = 0; n2 < 8; ++n2) {
+                x_lo[n2] = acc_lo[n2] * inv_q;
+                x_hi[n2] = acc_hi[n2] * inv_q;
+            }
+            double2* pk = dec + (size_t)ok * P * H + oa * H;
+#pragma unroll
+            for (int lvl = 0; lvl < L; ++lvl) {
+                double2 v[8];
+#pragma unroll
+                for (int n2 = 0; n2 < 8; ++n2) {
+                    const double ylo = x_lo[n2] * beta;
+                    const double dlo = rint(ylo);
+                    x_lo[n2] = ylo - dlo;
+                    const double yhi = x_hi[n2] * beta;
+                    const double dhi = rint(yhi);
+                    x_hi[n2] = yhi - dhi;
+                    const double2 w = qt[on1 + Q8 * n2];   // zeta^i
+                    v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
+                }
+                dft8<false>(v);
+                twiddle<8, Q8, false>(v, tw, on1);
+                double2* poly = pk + lvl * 2 * H;
+#pragma unroll
+                for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[k2];
+            }
+        }
+        __syncthreads();
+        forward_middle<LOGH, 1>(dec, K * P, tw, tid, nt);
+
+        // pointwise: out[a] = sum_m X^{r_m} * sum_bc BSK[g,a,bc,m] * DEC[bc]
+        {
+            const size_t gbase = (size_t)g * 2 * P * M * H;
+            for (int t = tid; t < K * H; t += nt) {
+                const int k = t % K;
+                const int p = t / K;
+                double2* pk = dec + (size_t)k * P * H;
+                double2 d[P];
+#pragma unroll
+                for (int bc = 0; bc < P; ++bc) d[bc] = pk[bc * H + swz(p)];
+                const int j = freq[p];
+                const int e = 4 * j + 1;                       // evaluation point zeta^e
+                // reference layout index of the same point (or its conjugate)
+                const bool cj = REFLAYOUT && (e >= N);
+                const int jr = REFLAYOUT ? (cj ? (N - 1 - 2 * j) : 2 * j) : p;
+                double2 o0 = make_double2(0.0, 0.0), o1 = make_double2(0.0, 0.0);
+                const int* rk = rot + k * M;
+                for (int m = 0; m < M; ++m) {
+                    double2 w;
+                    if constexpr (REFLAYOUT) {
+                        w = __ldg(args.all_rot + (size_t)rk[m] * H + jr);
+                        if (cj) w = c_conj(w);
+                    } else {
+                        w = root2n<LOGN>(qt, rk[m] * e);
+                    }
+                    double2 t0 = make_double2(0.0, 0.0), t1 = make_double2(0.0, 0.0);
+                    const double2* b0 = args.bsk + gbase + (size_t)m * H + jr;
+                    const double2* b1 = b0 + (size_t)P * M * H;
+#pragma unroll
+                    for (int bc = 0; bc < P; ++bc) {
+                        double2 k0 = __ldg(b0 + (size_t)bc * M * H);
+                        double2 k1 = __ldg(b1 + (size_t)bc * M * H);
+                        if (cj) { k0 = c_conj(k0); k1 = c_conj(k1); }
+                        c_mac(t0, k0, d[bc]);
+                        c_mac(t1, k1, d[bc]);
+                    }
+                    c_mac(o0, w, t0);
+                    c_mac(o1, w, t1);
+                }
+                pk[swz(p)] = o0;
+                pk[H + swz(p)] = o1;
+            }
+        }
+        __syncthreads();
+        inverse_middle<LOGH, PL::NS - 1>(dec, K, P, tw, tid, nt);
+
+        // last DIT superstage, untwist, round, centred reduction
+        {
+            double2* poly = dec + (size_t)ok * P * H + oa * H;
+            double2 v[8];
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2) v[k2] = poly[swz(on1 + Q8 * k2)];
+            twiddle<8, Q8, true>(v, tw, on1);
+            dft8<true>(v);
+#pragma unroll
+            for (int n2 = 0; n2 < 8; ++n2) {
+                const double2 u = c_mul(c_conj(qt[on1 + Q8 * n2]), v[n2]);
+                const double rlo = rint(u.x * inv_h);
+                const double rhi = rint(-u.y * inv_h);
+                acc_lo[n2] = rlo - q * rint(rlo * inv_q);
+                acc_hi[n2] = rhi - q * rint(rhi * inv_q);
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---------------------------------------------------------------- epilogue
+    if constexpr (REFLAYOUT) {
+        if (ct0 + ok < args.B) {
+            int64_t* dst = args.out_i64 + (ct0 + ok) * 2 * N + oa * N;
+#pragma unroll
+            for (int n2 = 0; n2 < 8; ++n2) {
+                dst[on1 + Q8 * n2] = __double2ll_rn(acc_lo[n2]);
+                dst[on1 + Q8 * n2 + H] = __double2ll_rn(acc_hi[n2]);
+            }
+        }
+    } else {
+        // ACC to shared memory as u32, then rotate by -b~ (RLWE_jax.py:295-297)
+        // and, for the PBS, extract n_lut LWEs (RLWE_jax.py:301-303)
+        uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);       // [K][2][N]
+        {
+            uint32_t* dst = acc + (size_t)ok * 2 * N + oa * N;
+#pragma unroll
+            for (int n2 = 0; n2 < 8; ++n2) {
+                dst[on1 + Q8 * n2] = (uint32_t)(long long)acc_lo[n2];
+                dst[on1 + Q8 * n2 + H] = (uint32_t)(long long)acc_hi[n2];
+            }
+        }
+        for (int k = tid; k < K; k += nt) {
+            const long long ct = min(ct0 + k, args.B - 1);
+            const double b = (double)(int32_t)args.lwe_b[ct];
+            bexp[k] = (int)(rint((2.0 * N * b) / (q * args.n_lut)) * args.n_lut);
+        }
+        __syncthreads();
+        const int kv = (int)min((long long)K, args.B - ct0);
+        if (args.acc_out) {
+            for (int t = tid; t < kv * 2 * N; t += nt) {
+                const int k = t / (2 * N);
+                const int rem = t - k * 2 * N;
+                const int a = rem / N;
+                const int i = rem - a * N;
+                args.acc_out[(ct0 + k) * 2 * N + rem] = ncoef<LOGN>(acc + (size_t)k * 2 * N + a * N, i + bexp[k]);
+            }
+        }
+        if (args.out_a) {
+            const int nl = args.n_lut;
+            for (int t = tid; t < kv * nl * N; t += nt) {
+                const int k = t / (nl * N);
+                const int rem = t - k * nl * N;
+                const int al = rem / N;
+                const int j = rem - al * N;
+                args.out_a[(ct0 + k) * nl * N + rem] = ncoef<LOGN>(acc + (size_t)k * 2 * N, al - j + bexp[k]);
+            }
+            for (int t = tid; t < kv * nl; t += nt) {
+                const int k = t / nl;
+                const int al = t - k * nl;
+                args.out_b[(ct0 + k) * nl + al] = ncoef<LOGN>(acc + (size_t)k * 2 * N + N, al + bexp[k]);
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Forward FFT of the coefficient-domain bootstrapping key into the device
+// layout [G][2 out][P][M][H] (position order), P = 2L, bc = level * 2 + in.
+// Source: uint32 (2 in = left/right, 2 out = mask/body, G*M, L, N), the
+// layout of get_boostrapping_key_collapse (schemas/RLWE_jax.py:162-197).
+// The reference transforms the same integers with jax_fourier and permutes
+// (nn_tfhe/activation.py:49-53, cuTFHE/multiply.py:81-86).
+// ----------------------------------------------------------------------------
+struct BskConvArgs {
+    const uint32_t* src;
+    double2* dst;
+    const double2* qt;
+    const double2* tw;
+    int G, M, L;
+    long long npoly;   // 2 * 2 * G * M * L
+};
+
+template <int LOGN>
+__global__ void __launch_bounds__(256) bsk_fft_kernel(const BskConvArgs a) {
+    constexpr int N = 1 << LOGN;
+    constexpr int H = N / 2;
+    constexpr int LOGH = LOGN - 1;
+    constexpr int PPC = (2048 / H) > 0 ? (2048 / H) : 1;   // polys per CTA (<= 32 KB)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long p0 = (long long)blockIdx.x * PPC;
+    const int P = 2 * a.L;
+    const long long GM = (long long)a.G * a.M;
+
+    for (int idx = tid; idx < PPC * H; idx += nt) {
+        const int lp = idx / H, i = idx % H;
+        const long long pi = min(p0 + lp, a.npoly - 1);
+        const uint32_t* s = a.src + pi * N;
+        const double lo = (double)(int32_t)s[i];
+        const double hi = (double)(int32_t)s[i + H];
+        const double2 w = a.qt[i];
+        buf[lp * H + swz(i)] = make_double2(fma(w.x, lo, w.y * hi), fma(w.y, lo, -w.x * hi));
+    }
+    __syncthreads();
+    forward_middle<LOGH, 0>(buf, PPC, a.tw, tid, nt);
+    for (int idx = tid; idx < PPC * H; idx += nt) {
+        const int lp = idx / H, p = idx % H;
+        const long long pi = p0 + lp;
+        if (pi >= a.npoly) continue;
+        const int lvl = (int)(pi % a.L);
+        const long long gm = (pi / a.L) % GM;
+        const int out = (int)((pi / (a.L * GM)) % 2);
+        const int in = (int)(pi / (2 * a.L * GM));
+        const long long g = gm / a.M;
+        const int m = (int)(gm % a.M);
+        const int bc = lvl * 2 + in;
+        a.dst[(((g * 2 + out) * P + bc) * a.M + m) * H + p] = buf[lp * H + swz(p)];
+    }
+}
+
+}  // namespace tfhe

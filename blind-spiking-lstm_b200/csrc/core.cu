@@ -1,0 +1,716 @@
+// C entry points, FFT plans, key upload, key switching and sample extraction
+// of the B200 TFHE PBS engine.  See include/tfhe_b200.h for the contract.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tfhe_b200.h"
+#include "tfhe_dispatch.h"
+#include "tfhe_internal.cuh"
+
+struct tfhe_keys {
+    tfhe_params p;
+    int device = -1;
+    int G = 0, M = 0;
+    double2* bsk = nullptr;     // [G][2][2L][M][N/2] FP64 Fourier, position order
+    uint32_t* ksk = nullptr;    // [n_big * l_ks][ldk]: columns 0..n-1 mask, n body
+    int ldk = 0;
+    const tfhe::FftPlan* plan = nullptr;
+    int64_t bytes = 0;
+};
+
+namespace tfhe {
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return TFHE_OK;
+    const std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return fail(TFHE_ERR_OUT_OF_MEMORY, msg);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return fail(TFHE_ERR_NO_DEVICE, msg);
+    return fail(TFHE_ERR_INTERNAL, msg);
+}
+
+#define TFHE_TRY(expr)                          \
+    do {                                        \
+        const int _rc = (expr);                 \
+        if (_rc != TFHE_OK) return _rc;         \
+    } while (0)
+
+// ---------------------------------------------------------------- FFT plans
+static int ilog2(long long v) {
+    int r = -1;
+    while (v) { v >>= 1; ++r; }
+    return r;
+}
+
+static bool is_pow2(long long v) { return v > 0 && (v & (v - 1)) == 0; }
+
+// radix sequence of an H = 2^logh point transform (same as Plan<LOGH>)
+static std::vector<int> radices(int logh) {
+    std::vector<int> r(logh / 3, 8);
+    if (logh % 3 == 1) r.push_back(2);
+    if (logh % 3 == 2) r.push_back(4);
+    return r;
+}
+
+int plan_tw_count(int logh) {
+    const std::vector<int> r = radices(logh);
+    const int H = 1 << logh;
+    int prod = 1, total = 0;
+    for (int R : r) {
+        prod *= R;
+        total += (R - 1) * (H / prod);
+    }
+    return total;
+}
+
+// exp(-i pi k / N) with the angle reduced in long double
+static double2 root(long long k, int N) {
+    k %= 2LL * N;
+    if (k < 0) k += 2LL * N;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    const long double ang = pi * (long double)k / (long double)N;
+    return make_double2((double)cosl(ang), (double)(-sinl(ang)));
+}
+
+static void build_tables(int N, std::vector<double2>& qt, std::vector<double2>& tw, std::vector<uint16_t>& freq) {
+    const int H = N / 2;
+    const int logh = ilog2(H);
+    qt.resize(N / 2);
+    for (int r = 0; r < N / 2; ++r) qt[r] = root(r, N);
+    const std::vector<int> rs = radices(logh);
+    tw.clear();
+    int prod = 1;
+    for (int R : rs) {
+        prod *= R;
+        const int S = H / prod;
+        for (int k2 = 1; k2 < R; ++k2)
+            for (int n1 = 0; n1 < S; ++n1)
+                tw.push_back(root((long long)(2 * N / (R * S)) * n1 * k2, N));
+    }
+    // frequency of position p: p = S1 * k2 + pos_{S1}(k1) for k = R1 k1 + k2
+    freq.resize(H);
+    for (int p = 0; p < H; ++p) {
+        int rem = p, size = H, mult = 1, k = 0;
+        for (int R : rs) {
+            const int S = size / R;
+            const int k2 = rem / S;
+            k += mult * k2;
+            mult *= R;
+            rem %= S;
+            size = S;
+        }
+        freq[p] = (uint16_t)k;
+    }
+}
+
+static std::mutex g_plan_mu;
+static std::map<std::pair<int, int>, FftPlan*> g_plans;   // (device, N)
+
+const FftPlan* get_plan(int N) {
+    int dev = 0;
+    if (check_cuda(cudaGetDevice(&dev), "cudaGetDevice") != TFHE_OK) return nullptr;
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plans.find({dev, N});
+    if (it != g_plans.end()) return it->second;
+    std::vector<double2> qt, tw;
+    std::vector<uint16_t> freq;
+    build_tables(N, qt, tw, freq);
+    FftPlan* pl = new FftPlan();
+    pl->N = N;
+    pl->tw_count = (int)tw.size();
+    bool ok = cudaMalloc(&pl->qt, qt.size() * sizeof(double2)) == cudaSuccess &&
+              cudaMalloc(&pl->tw, tw.size() * sizeof(double2)) == cudaSuccess &&
+              cudaMalloc(&pl->freq, freq.size() * sizeof(uint16_t)) == cudaSuccess &&
+              cudaMemcpy(pl->qt, qt.data(), qt.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(pl->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(pl->freq, freq.data(), freq.size() * sizeof(uint16_t), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+        set_error("FFT plan upload failed: " + std::string(cudaGetErrorString(cudaGetLastError())));
+        cudaFree(pl->qt);
+        cudaFree(pl->tw);
+        cudaFree(pl->freq);
+        delete pl;
+        return nullptr;
+    }
+    g_plans[{dev, N}] = pl;
+    return pl;
+}
+
+size_t br_table_bytes(int N) {
+    const int H = N / 2;
+    return (size_t)(N / 2) * sizeof(double2) + (size_t)plan_tw_count(ilog2(H)) * sizeof(double2) +
+           (size_t)H * sizeof(uint16_t);
+}
+
+static int max_smem_optin() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 48 * 1024;
+    if (!cached[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0)
+            v = 48 * 1024;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
+// ---------------------------------------------------------------- BR launch
+struct BrShape {
+    int K = 0, nt = 0;
+    size_t smem = 0;
+};
+
+static BrShape br_shape(int N, int L, int M, long long B) {
+    const int H = N / 2, Q8 = H / 8;
+    const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
+    const size_t limit = (size_t)max_smem_optin();
+    BrShape s;
+    int K = std::max(1, 512 / (2 * Q8));
+    K = (int)std::min<long long>(K, std::max<long long>(B, 1));
+    while (K >= 1) {
+        const size_t smem = per_ct * K + br_table_bytes(N) + (size_t)(K * M + K) * sizeof(int) + 16;
+        if (smem <= limit) {
+            s.K = K;
+            s.nt = K * 2 * Q8;
+            s.smem = smem;
+            return s;
+        }
+        --K;
+    }
+    return s;
+}
+
+static int launch_br(BrArgs args, int N, int L, bool reflayout, cudaStream_t stream) {
+    const int logn = ilog2(N);
+    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout);
+    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
+    const BrShape sh = br_shape(N, L, args.M, args.B);
+    if (sh.K < 1)
+        return fail(TFHE_ERR_INVALID_ARGUMENT,
+                    "degree " + std::to_string(N) + " with l=" + std::to_string(L) +
+                        " does not fit in shared memory");
+    const FftPlan* pl = get_plan(N);
+    if (!pl) return TFHE_ERR_INTERNAL;
+    args.qt = pl->qt;
+    args.tw = pl->tw;
+    args.freq = pl->freq;
+    args.K = sh.K;
+    TFHE_TRY(check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sh.smem),
+                        "cudaFuncSetAttribute(blind rotation)"));
+    const long long grid = (args.B + sh.K - 1) / sh.K;
+    kern<<<(unsigned)grid, sh.nt, sh.smem, stream>>>(args);
+    return check_cuda(cudaGetLastError(), "blind rotation launch");
+}
+
+// ---------------------------------------------------------------- key switch
+// out[k][o] = sum_{i,j} d_j(a[k][i]) KSK[i*l + j][o] (mod 2^32); o = n is the
+// body column (added to b).  Digits are the float64 steps of
+// decomposition (schemas/polynomial_jax.py:98-111) at base 2^log2_beta_ks.
+constexpr int KS_TB = 64, KS_TO = 64, KS_KC = 8, KS_LMAX = 8;
+
+// Key rows are addressed by strides so the device layout and the
+// reference layout (mask (l, n_big, n), body (l, n_big)) share the kernel:
+// mask(i, j, o) = ka[i*si + j*sj + o], body(i, j) = kb[i*bi + j*bj].
+struct KsKey {
+    const uint32_t* ka;
+    const uint32_t* kb;
+    long long si, sj, bi, bj;
+};
+
+__global__ void __launch_bounds__(256) ks_kernel(const uint32_t* __restrict__ a_in,
+                                                 const uint32_t* __restrict__ b_in, const KsKey key,
+                                                 int n_big, int n, int l, int log2_beta,
+                                                 uint32_t* __restrict__ a_out, uint32_t* __restrict__ b_out,
+                                                 long long B) {
+    __shared__ int dig[KS_TB][KS_KC * KS_LMAX + 1];
+    __shared__ __align__(16) uint32_t kt[KS_KC * KS_LMAX][KS_TO];
+    const int tid = threadIdx.x;
+    const int ty = tid / 16, tx = tid % 16;
+    const long long r0 = (long long)blockIdx.y * KS_TB;
+    const int o0 = blockIdx.x * KS_TO;
+    const double inv_q = ldexp(1.0, -32);
+    const double beta = ldexp(1.0, log2_beta);
+    uint32_t acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0u;
+
+    for (int i0 = 0; i0 < n_big; i0 += KS_KC) {
+        for (int idx = tid; idx < KS_TB * KS_KC; idx += 256) {
+            const int ct = idx / KS_KC, c = idx % KS_KC;
+            const long long row = r0 + ct;
+            const int i = i0 + c;
+            const uint32_t v = (row < B && i < n_big) ? a_in[row * n_big + i] : 0u;
+            double x = (double)(int32_t)v * inv_q;
+            for (int j = 0; j < l; ++j) {
+                const double y = x * beta;
+                const double d = rint(y);
+                x = y - d;
+                dig[ct][c * l + j] = (int)d;
+            }
+        }
+        const int rows = KS_KC * l;
+        for (int idx = tid; idx < rows * KS_TO; idx += 256) {
+            const int r = idx / KS_TO, col = idx % KS_TO;
+            const int i = i0 + r / l, j = r % l;
+            const int o = o0 + col;
+            uint32_t v = 0u;
+            if (i < n_big) {
+                if (o < n) v = key.ka[i * key.si + j * key.sj + o];
+                else if (o == n) v = key.kb[i * key.bi + j * key.bj];
+            }
+            kt[r][col] = v;
+        }
+        __syncthreads();
+        for (int r = 0; r < rows; ++r) {
+            const uint4 kv = *reinterpret_cast<const uint4*>(&kt[r][tx * 4]);
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                const uint32_t d = (uint32_t)dig[ty * 4 + cc][r];
+                acc[cc][0] += d * kv.x;
+                acc[cc][1] += d * kv.y;
+                acc[cc][2] += d * kv.z;
+                acc[cc][3] += d * kv.w;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+        const long long row = r0 + ty * 4 + cc;
+        if (row >= B) continue;
+#pragma unroll
+        for (int oo = 0; oo < 4; ++oo) {
+            const int o = o0 + tx * 4 + oo;
+            if (o < n) a_out[row * n + o] = acc[cc][oo];
+            else if (o == n) b_out[row] = b_in[row] + acc[cc][oo];
+        }
+    }
+}
+
+static int launch_ks_key(const KsKey& key, int n_big, int n, int l, int log2_beta, const uint32_t* a_in,
+                         const uint32_t* b_in, uint32_t* a_out, uint32_t* b_out, long long B, cudaStream_t stream) {
+    if (B == 0) return TFHE_OK;
+    const dim3 grid((n + 1 + KS_TO - 1) / KS_TO, (unsigned)((B + KS_TB - 1) / KS_TB));
+    ks_kernel<<<grid, 256, 0, stream>>>(a_in, b_in, key, n_big, n, l, log2_beta, a_out, b_out, B);
+    return check_cuda(cudaGetLastError(), "key switch launch");
+}
+
+static int launch_ks(const tfhe_keys* k, const uint32_t* a_in, const uint32_t* b_in, uint32_t* a_out,
+                     uint32_t* b_out, long long B, cudaStream_t stream) {
+    const long long ldk = k->ldk, l = k->p.l_ks;
+    const KsKey key{k->ksk, k->ksk + k->p.n, l * ldk, ldk, l * ldk, ldk};
+    return launch_ks_key(key, k->p.n_big, k->p.n, k->p.l_ks, k->p.log2_beta_ks, a_in, b_in, a_out, b_out, B,
+                         stream);
+}
+
+// ---------------------------------------------------------------- extraction
+// out_a[k][al][j] = coefficient of X^(al - j) of the mask (negacyclic),
+// out_b[k][al] = body[al]  (schemas/text_jax.py:191-208)
+__global__ void extract_kernel(const uint32_t* __restrict__ acc, int N, int n_lut, uint32_t* __restrict__ out_a,
+                               uint32_t* __restrict__ out_b, long long B) {
+    const long long total = B * n_lut * (long long)N;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long k = t / ((long long)n_lut * N);
+        const int rem = (int)(t - k * n_lut * (long long)N);
+        const int al = rem / N, j = rem % N;
+        const uint32_t* a = acc + k * 2 * N;
+        const int e = al - j;
+        out_a[t] = e >= 0 ? a[e] : (0u - a[e + N]);
+        if (j == 0) out_b[k * n_lut + al] = a[N + al];
+    }
+}
+
+// rotation by -b~ then many-LUT extraction on int64 values of the reference
+// (schemas/RLWE_jax.py:295-303), keeping its +-q/2 representatives
+__global__ void rotate_extract_i64_kernel(const int64_t* __restrict__ acc, const double* __restrict__ b, int N,
+                                          int n_lut, double q, int64_t* __restrict__ out_acc,
+                                          int64_t* __restrict__ out_a, int64_t* __restrict__ out_b, long long B) {
+    const long long per = 2LL * N + (long long)n_lut * N + n_lut;
+    const long long total = B * per;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long k = t / per;
+        const int r = (int)(t - k * per);
+        const int bt = (int)(rint((2.0 * N * b[k]) / (q * n_lut)) * n_lut);
+        const int64_t* a = acc + k * 2 * N;
+        int e, src;
+        int64_t* dst;
+        if (r < 2 * N) {                        // rotated ACC
+            if (!out_acc) continue;
+            const int comp = r / N;
+            e = (r % N) + bt;
+            src = comp * N;
+            dst = out_acc + k * 2 * N + r;
+        } else if (r < 2 * N + n_lut * N) {     // extracted masks
+            if (!out_a) continue;
+            const int rr = r - 2 * N;
+            const int al = rr / N, j = rr % N;
+            e = al - j + bt;
+            src = 0;
+            dst = out_a + k * (long long)n_lut * N + rr;
+        } else {                                // extracted bodies
+            if (!out_b) continue;
+            const int al = r - 2 * N - n_lut * N;
+            e = al + bt;
+            src = N;
+            dst = out_b + k * n_lut + al;
+        }
+        e %= 2 * N;
+        if (e < 0) e += 2 * N;
+        *dst = e < N ? a[src + e] : -a[src + e - N];
+    }
+}
+
+// ---------------------------------------------------------------- validation
+static int validate_params(const tfhe_params* p) {
+    if (!p) return fail(TFHE_ERR_INVALID_ARGUMENT, "params is NULL");
+    if (!is_pow2(p->N) || p->N < 128 || p->N > 4096) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree N");
+    if (p->l_bs < 1 || p->l_bs > 4) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported l_bs (1..4)");
+    if (p->collapse < 1 || p->collapse > 4) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported collapse (1..4)");
+    if (p->n <= 0 || p->n % p->collapse) return fail(TFHE_ERR_INVALID_ARGUMENT, "n must be a positive multiple of collapse");
+    if (p->n_big <= 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_big must be positive");
+    if (p->log2_q != 32) return fail(TFHE_ERR_INVALID_ARGUMENT, "native entry points need log2_q == 32");
+    if (p->log2_beta_bs < 1 || p->log2_beta_bs * p->l_bs > 32)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "log2_beta_bs * l_bs must be in [1, 32]");
+    if (p->l_ks < 1 || p->l_ks > KS_LMAX || p->log2_beta_ks < 1 || p->log2_beta_ks * p->l_ks > 32)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported key-switch base / levels");
+    if (br_shape(p->N, p->l_bs, 1 << p->collapse, 1).K < 1)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "degree / levels do not fit in shared memory");
+    return TFHE_OK;
+}
+
+static int check_keys(const tfhe_keys* k) {
+    if (!k) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys is NULL");
+    int dev = -1;
+    TFHE_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+    if (dev != k->device)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "keys live on device " + std::to_string(k->device) +
+                                                   " but device " + std::to_string(dev) + " is current");
+    return TFHE_OK;
+}
+
+static int upload_ksk(tfhe_keys* k, const uint32_t* ksk_a, const uint32_t* ksk_b, cudaStream_t stream) {
+    const tfhe_params& p = k->p;
+    k->ldk = (p.n + 1 + 3) / 4 * 4;
+    const size_t rows = (size_t)p.n_big * p.l_ks;
+    std::vector<uint32_t> host(rows * k->ldk, 0u);
+    for (int j = 0; j < p.l_ks; ++j)
+        for (int i = 0; i < p.n_big; ++i) {
+            uint32_t* dst = host.data() + ((size_t)i * p.l_ks + j) * k->ldk;
+            std::memcpy(dst, ksk_a + ((size_t)j * p.n_big + i) * p.n, (size_t)p.n * sizeof(uint32_t));
+            dst[p.n] = ksk_b[(size_t)j * p.n_big + i];
+        }
+    const size_t bytes = host.size() * sizeof(uint32_t);
+    TFHE_TRY(check_cuda(cudaMalloc(&k->ksk, bytes), "cudaMalloc(ksk)"));
+    k->bytes += (int64_t)bytes;
+    TFHE_TRY(check_cuda(cudaMemcpyAsync(k->ksk, host.data(), bytes, cudaMemcpyHostToDevice, stream), "ksk upload"));
+    return check_cuda(cudaStreamSynchronize(stream), "ksk upload sync");
+}
+
+static int keys_common(const tfhe_params* params, tfhe_keys** out, tfhe_keys** made) {
+    if (!out) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys_out is NULL");
+    *out = nullptr;
+    TFHE_TRY(validate_params(params));
+    tfhe_keys* k = new tfhe_keys();
+    k->p = *params;
+    k->G = params->n / params->collapse;
+    k->M = 1 << params->collapse;
+    if (check_cuda(cudaGetDevice(&k->device), "cudaGetDevice") != TFHE_OK) {
+        delete k;
+        return TFHE_ERR_NO_DEVICE;
+    }
+    k->plan = get_plan(params->N);
+    if (!k->plan) {
+        delete k;
+        return TFHE_ERR_INTERNAL;
+    }
+    *made = k;
+    return TFHE_OK;
+}
+
+static void keys_free(tfhe_keys* k) {
+    if (!k) return;
+    cudaFree(k->bsk);
+    cudaFree(k->ksk);
+    delete k;
+}
+
+}  // namespace tfhe
+
+using namespace tfhe;
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* tfhe_version(void) { return "tfhe_b200 1 (sm_100a, FP64 batched blind rotation)"; }
+
+const char* tfhe_last_error(void) { return g_last_error.c_str(); }
+
+int tfhe_mul_bootstrap(void* stream, const int64_t* ct_init, int64_t ct_elems, const void* bsk,
+                       const int64_t* bsk_dims, const void* all_rot_fft, int64_t all_rot_rows,
+                       const int32_t* indices, int64_t log2_beta, int64_t log2_q, int64_t l, int64_t degree,
+                       int64_t* out, int64_t batch) {
+    switch (degree) {
+        case 128: case 256: case 512: case 1024: case 2048: case 4096: break;
+        default: return fail(TFHE_ERR_INVALID_ARGUMENT, "Unsupported degree");
+    }
+    if (l < 1 || l > 4) return fail(TFHE_ERR_INVALID_ARGUMENT, "Unsupported l");
+    if (!bsk_dims) return fail(TFHE_ERR_INVALID_ARGUMENT, "bsk_dims is NULL");
+    const int64_t G = bsk_dims[0], A = bsk_dims[1], Lb = bsk_dims[2], C = bsk_dims[3], M = bsk_dims[4],
+                  D = bsk_dims[5];
+    if (A != 2 || C != 2 || Lb != l || D != degree / 2 || M < 1 || M > 16 || !is_pow2(M) || G < 1)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "bsk must be (G, 2, l, 2, M, degree/2) with M a power of two <= 16");
+    if (all_rot_rows != 2 * degree) return fail(TFHE_ERR_INVALID_ARGUMENT, "all_rot_fft must have 2*degree rows");
+    if (log2_q < 2 || log2_q > 64 || log2_beta < 1 || log2_beta > 62)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported log2_q / log2_beta");
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (ct_elems != 2 * degree && ct_elems != 2 * degree * batch)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "ct_init must hold 2N or batch*2N elements");
+    if (batch == 0) return TFHE_OK;
+    if (!ct_init || !bsk || !all_rot_fft || !indices || !out)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    BrArgs a{};
+    a.bsk = static_cast<const double2*>(bsk);
+    a.all_rot = static_cast<const double2*>(all_rot_fft);
+    a.G = (int)G;
+    a.M = (int)M;
+    a.collapse = ilog2(M);
+    a.B = batch;
+    a.log2_beta = (int)log2_beta;
+    a.log2_q = (int)log2_q;
+    a.ct_init = ct_init;
+    a.ct_stride = (ct_elems > 2 * degree) ? 2 * degree : 0;
+    a.indices = indices;
+    a.out_i64 = out;
+    a.n_lut = 1;
+    return launch_br(a, (int)degree, (int)l, true, static_cast<cudaStream_t>(stream));
+}
+
+int tfhe_keys_create(const tfhe_params* params, const uint32_t* bsk_coeff, const uint32_t* ksk_a,
+                     const uint32_t* ksk_b, void* stream_v, tfhe_keys** keys_out) {
+    tfhe_keys* k = nullptr;
+    TFHE_TRY(keys_common(params, keys_out, &k));
+    if (!bsk_coeff || !ksk_a || !ksk_b) {
+        keys_free(k);
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL key buffer");
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    const tfhe_params& p = *params;
+    const int N = p.N, H = N / 2, L = p.l_bs;
+    const long long npoly = 4LL * k->G * k->M * L;
+    const size_t src_bytes = (size_t)npoly * N * sizeof(uint32_t);
+    const size_t dst_bytes = (size_t)npoly * H * sizeof(double2);
+    uint32_t* d_src = nullptr;
+    int rc = check_cuda(cudaMalloc(&d_src, src_bytes), "cudaMalloc(bsk staging)");
+    if (rc == TFHE_OK) rc = check_cuda(cudaMalloc(&k->bsk, dst_bytes), "cudaMalloc(bsk)");
+    if (rc == TFHE_OK) {
+        k->bytes += (int64_t)dst_bytes;
+        rc = check_cuda(cudaMemcpyAsync(d_src, bsk_coeff, src_bytes, cudaMemcpyHostToDevice, stream), "bsk upload");
+    }
+    if (rc == TFHE_OK) {
+        BskConvArgs ca{d_src, k->bsk, k->plan->qt, k->plan->tw, k->G, k->M, L, npoly};
+        const int ppc = std::max(1, 2048 / H);
+        const size_t smem = (size_t)ppc * H * sizeof(double2);
+        BrConvKernel kern = bsk_fft_kernel_for(ilog2(N));
+        rc = check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                        "cudaFuncSetAttribute(bsk fft)");
+        if (rc == TFHE_OK) {
+            kern<<<(unsigned)((npoly + ppc - 1) / ppc), 256, smem, stream>>>(ca);
+            rc = check_cuda(cudaGetLastError(), "bsk fft launch");
+        }
+        if (rc == TFHE_OK) rc = check_cuda(cudaStreamSynchronize(stream), "bsk fft");
+    }
+    cudaFree(d_src);
+    if (rc == TFHE_OK) rc = upload_ksk(k, ksk_a, ksk_b, stream);
+    if (rc != TFHE_OK) {
+        keys_free(k);
+        return rc;
+    }
+    *keys_out = k;
+    return TFHE_OK;
+}
+
+int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordered, const uint32_t* ksk_a,
+                             const uint32_t* ksk_b, void* stream_v, tfhe_keys** keys_out) {
+    tfhe_keys* k = nullptr;
+    TFHE_TRY(keys_common(params, keys_out, &k));
+    if (!bsk_ordered || !ksk_a || !ksk_b) {
+        keys_free(k);
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL key buffer");
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    const tfhe_params& p = *params;
+    const int N = p.N, H = N / 2, L = p.l_bs, P = 2 * L, G = k->G, M = k->M;
+    std::vector<double2> qt, tw;
+    std::vector<uint16_t> freq;
+    build_tables(N, qt, tw, freq);
+    // bsk_ordered (2 out, 2 in, L, G*M, H) at zeta^(2j+1) -> [G][2][P][M][H]
+    // at zeta^(4 freq[p] + 1) (the point or the conjugate of its partner)
+    const size_t total = (size_t)G * 2 * P * M * H;
+    std::vector<double2> host(total);
+    const double2* src = reinterpret_cast<const double2*>(bsk_ordered);
+    for (int g = 0; g < G; ++g)
+        for (int a = 0; a < 2; ++a)
+            for (int lvl = 0; lvl < L; ++lvl)
+                for (int c = 0; c < 2; ++c)
+                    for (int m = 0; m < M; ++m) {
+                        const double2* row = src + ((((size_t)a * 2 + c) * L + lvl) * ((size_t)G * M) + (size_t)g * M + m) * H;
+                        double2* dst = host.data() + ((((size_t)g * 2 + a) * P + lvl * 2 + c) * M + m) * H;
+                        for (int pp = 0; pp < H; ++pp) {
+                            const int j = freq[pp];
+                            const int e = 4 * j + 1;
+                            dst[pp] = e < N ? row[2 * j] : make_double2(row[N - 1 - 2 * j].x, -row[N - 1 - 2 * j].y);
+                        }
+                    }
+    int rc = check_cuda(cudaMalloc(&k->bsk, total * sizeof(double2)), "cudaMalloc(bsk)");
+    if (rc == TFHE_OK) {
+        k->bytes += (int64_t)(total * sizeof(double2));
+        rc = check_cuda(cudaMemcpyAsync(k->bsk, host.data(), total * sizeof(double2), cudaMemcpyHostToDevice, stream),
+                        "bsk upload");
+    }
+    if (rc == TFHE_OK) rc = check_cuda(cudaStreamSynchronize(stream), "bsk upload sync");
+    if (rc == TFHE_OK) rc = upload_ksk(k, ksk_a, ksk_b, stream);
+    if (rc != TFHE_OK) {
+        keys_free(k);
+        return rc;
+    }
+    *keys_out = k;
+    return TFHE_OK;
+}
+
+void tfhe_keys_destroy(tfhe_keys* keys) { keys_free(keys); }
+
+int64_t tfhe_keys_device_bytes(const tfhe_keys* keys) { return keys ? keys->bytes : 0; }
+
+int tfhe_keyswitch(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, uint32_t* a_out,
+                   uint32_t* b_out, int64_t batch, void* stream) {
+    TFHE_TRY(check_keys(keys));
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch > 0 && (!a_in || !b_in || !a_out || !b_out)) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    return launch_ks(keys, a_in, b_in, a_out, b_out, batch, static_cast<cudaStream_t>(stream));
+}
+
+static int br_native(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
+                     int64_t lut_count, int32_t n_lut, uint32_t* acc_out, uint32_t* out_a, uint32_t* out_b,
+                     int64_t batch, cudaStream_t stream) {
+    const tfhe_params& p = keys->p;
+    if (n_lut < 1 || n_lut > p.N) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut must be in [1, N]");
+    if (lut_count != 1 && lut_count != batch) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut_count must be 1 or batch");
+    BrArgs a{};
+    a.bsk = keys->bsk;
+    a.G = keys->G;
+    a.M = keys->M;
+    a.collapse = p.collapse;
+    a.B = batch;
+    a.log2_beta = p.log2_beta_bs;
+    a.log2_q = 32;
+    a.lwe_a = lwe_a;
+    a.lwe_b = lwe_b;
+    a.lut = lut;
+    a.lut_stride = lut_count == 1 ? 0 : 2LL * p.N;
+    a.n_lut = n_lut;
+    a.lwe_n = p.n;
+    a.acc_out = acc_out;
+    a.out_a = out_a;
+    a.out_b = out_b;
+    return launch_br(a, p.N, p.l_bs, false, stream);
+}
+
+int tfhe_blind_rotate(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
+                      int64_t lut_count, int32_t n_lut, uint32_t* acc_out, int64_t batch, void* stream) {
+    TFHE_TRY(check_keys(keys));
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!lwe_a || !lwe_b || !lut || !acc_out) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    return br_native(keys, lwe_a, lwe_b, lut, lut_count, n_lut, acc_out, nullptr, nullptr, batch,
+                     static_cast<cudaStream_t>(stream));
+}
+
+int tfhe_sample_extract(const uint32_t* acc, int32_t N, int32_t n_lut, uint32_t* out_a, uint32_t* out_b,
+                        int64_t batch, void* stream) {
+    if (!is_pow2(N) || N < 2) return fail(TFHE_ERR_INVALID_ARGUMENT, "N must be a power of two");
+    if (n_lut < 1 || n_lut > N) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut must be in [1, N]");
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!acc || !out_a || !out_b) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    const long long total = batch * (long long)n_lut * N;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+    extract_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(acc, N, n_lut, out_a, out_b, batch);
+    return check_cuda(cudaGetLastError(), "sample extract launch");
+}
+
+int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, const uint32_t* lut,
+             int64_t lut_count, int32_t n_lut, uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream_v) {
+    TFHE_TRY(check_keys(keys));
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!a_in || !b_in || !lut || !out_a || !out_b) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    const size_t n = (size_t)keys->p.n;
+    uint32_t* ks = nullptr;
+    TFHE_TRY(check_cuda(cudaMallocAsync(&ks, (size_t)batch * (n + 1) * sizeof(uint32_t), stream),
+                        "cudaMallocAsync(key-switch output)"));
+    uint32_t* ks_b = ks + (size_t)batch * n;
+    int rc = launch_ks(keys, a_in, b_in, ks, ks_b, batch, stream);
+    if (rc == TFHE_OK)
+        rc = br_native(keys, ks, ks_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch, stream);
+    const int rc2 = check_cuda(cudaFreeAsync(ks, stream), "cudaFreeAsync(key-switch output)");
+    return rc != TFHE_OK ? rc : rc2;
+}
+
+int tfhe_keyswitch_ref(const uint32_t* a_in, const uint32_t* b_in, const uint32_t* ksk_a, const uint32_t* ksk_b,
+                       int32_t n_big, int32_t n, int32_t l_ks, int32_t log2_beta_ks, uint32_t* a_out,
+                       uint32_t* b_out, int64_t batch, void* stream) {
+    if (n_big <= 0 || n <= 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "dimensions must be positive");
+    if (l_ks < 1 || l_ks > KS_LMAX || log2_beta_ks < 1 || log2_beta_ks * l_ks > 32)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported key-switch base / levels");
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!a_in || !b_in || !ksk_a || !ksk_b || !a_out || !b_out) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    const KsKey key{ksk_a, ksk_b, n, (long long)n_big * n, 1, n_big};
+    return launch_ks_key(key, n_big, n, l_ks, log2_beta_ks, a_in, b_in, a_out, b_out, batch,
+                         static_cast<cudaStream_t>(stream));
+}
+
+int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int32_t n_lut, int64_t log2_q,
+                            int64_t* out_acc, int64_t* out_a, int64_t* out_b, int64_t batch, void* stream) {
+    if (!is_pow2(N) || N < 2) return fail(TFHE_ERR_INVALID_ARGUMENT, "N must be a power of two");
+    if (n_lut < 1 || n_lut > N) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut must be in [1, N]");
+    if (log2_q < 2 || log2_q > 64) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported log2_q");
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!acc || !b || (!out_acc && !out_a && !out_b) || ((out_a == nullptr) != (out_b == nullptr)))
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    const long long total = batch * (2LL * N + (long long)n_lut * N + n_lut);
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+    rotate_extract_i64_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        acc, b, N, n_lut, std::ldexp(1.0, (int)log2_q), out_acc, out_a, out_b, batch);
+    return check_cuda(cudaGetLastError(), "rotate/extract launch");
+}
+
+}  // extern "C"

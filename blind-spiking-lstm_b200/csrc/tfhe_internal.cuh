@@ -1,0 +1,244 @@
+// Internal declarations of the B200 TFHE programmable-bootstrapping engine.
+//
+// Polynomials of Z_q[X]/(X^N+1) are carried in the "folded" negacyclic
+// Fourier domain: a real polynomial p of degree N is evaluated at the N/2
+// points zeta^(4j+1), zeta = exp(-i*pi/N), j in [0, N/2), through one
+// H = N/2 point complex FFT of z_k = zeta^k (p_k - i p_{k+H}).  Those points
+// hold one root of every conjugate pair, so pointwise products in this
+// domain are negacyclic products.  The FFT is decimation-in-frequency
+// (forward) / decimation-in-time (inverse) without reordering: Fourier
+// values live in "position" order p, with frequency j = freq[p]
+// (mixed-radix digit reversal), and every key stored on the device uses
+// the same order so the pointwise stage never permutes.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <mutex>
+#include <string>
+
+namespace tfhe {
+
+// ----------------------------------------------------------------------------
+// status handling shared by the C entry points
+// ----------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int check_cuda(cudaError_t e, const char* what);
+
+// ----------------------------------------------------------------------------
+// complex helpers (double2 as re, im)
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 c_conj(double2 a) { return make_double2(a.x, -a.y); }
+// acc += a * b
+__device__ __forceinline__ void c_mac(double2& acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+}
+// multiply by -i, +i
+__device__ __forceinline__ double2 c_mul_mi(double2 a) { return make_double2(a.y, -a.x); }
+__device__ __forceinline__ double2 c_mul_pi(double2 a) { return make_double2(-a.y, a.x); }
+
+// ----------------------------------------------------------------------------
+// radix plan: H = 2^h points as radix-8 superstages then one radix-2 or -4
+// ----------------------------------------------------------------------------
+template <int LOGH>
+struct Plan {
+    static constexpr int H = 1 << LOGH;
+    static constexpr int N8 = LOGH / 3;             // radix-8 superstages
+    static constexpr int REM = LOGH % 3;            // 0, 1 (radix 2) or 2 (radix 4)
+    static constexpr int NS = N8 + (REM ? 1 : 0);   // superstages
+    static constexpr int radix(int s) { return s < N8 ? 8 : (REM == 1 ? 2 : 4); }
+    // span of superstage s (elements between the inputs of one butterfly)
+    static constexpr int span(int s) {
+        int prod = 1;
+        for (int i = 0; i <= s; ++i) prod *= radix(i);
+        return H / prod;
+    }
+    // offset of superstage s's twiddle table (R-1 rows of span entries)
+    static constexpr int tw_offset(int s) {
+        int off = 0;
+        for (int i = 0; i < s; ++i) off += (radix(i) - 1) * span(i);
+        return off;
+    }
+    static constexpr int TW = tw_offset(NS);        // total per-stage twiddles
+};
+
+// XOR swizzle of 16-byte elements inside 128-byte rows: strided butterfly
+// accesses of every superstage hit distinct bank groups.
+__device__ __forceinline__ int swz(int e) { return e ^ ((e >> 3) & 7); }
+
+// exp(-i pi idx / N) for any idx, from the quarter table qt[r] =
+// exp(-i pi r / N), r in [0, N/2)
+template <int LOGN>
+__device__ __forceinline__ double2 root2n(const double2* qt, int idx) {
+    constexpr int N = 1 << LOGN;
+    idx &= (2 * N - 1);
+    const int quad = idx >> (LOGN - 1);
+    const double2 w = qt[idx & (N / 2 - 1)];
+    switch (quad) {
+        case 0: return w;
+        case 1: return make_double2(w.y, -w.x);
+        case 2: return make_double2(-w.x, -w.y);
+        default: return make_double2(-w.y, w.x);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// small DFTs in registers, natural order in and out
+// ----------------------------------------------------------------------------
+template <bool INV>
+__device__ __forceinline__ void dft2(double2& a, double2& b) {
+    const double2 t = a;
+    a = c_add(t, b);
+    b = c_sub(t, b);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(double2 (&v)[4]) {
+    double2 a0 = c_add(v[0], v[2]), a2 = c_sub(v[0], v[2]);
+    double2 a1 = c_add(v[1], v[3]), a3 = c_sub(v[1], v[3]);
+    a3 = INV ? c_mul_pi(a3) : c_mul_mi(a3);
+    v[0] = c_add(a0, a1);
+    v[2] = c_sub(a0, a1);
+    v[1] = c_add(a2, a3);
+    v[3] = c_sub(a2, a3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(double2 (&v)[8]) {
+    constexpr double R2 = 0.70710678118654752440084436210485;
+    // span-4 butterflies with exp(-+2 pi i n / 8)
+    double2 a[8];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        a[n] = c_add(v[n], v[n + 4]);
+        a[n + 4] = c_sub(v[n], v[n + 4]);
+    }
+    if (!INV) {
+        a[5] = make_double2(R2 * (a[5].x + a[5].y), R2 * (a[5].y - a[5].x));
+        a[6] = c_mul_mi(a[6]);
+        a[7] = make_double2(R2 * (a[7].y - a[7].x), -R2 * (a[7].x + a[7].y));
+    } else {
+        a[5] = make_double2(R2 * (a[5].x - a[5].y), R2 * (a[5].x + a[5].y));
+        a[6] = c_mul_pi(a[6]);
+        a[7] = make_double2(-R2 * (a[7].x + a[7].y), R2 * (a[7].x - a[7].y));
+    }
+    // span-2 butterflies on each half with exp(-+2 pi i n / 4)
+    double2 b[8];
+#pragma unroll
+    for (int h = 0; h < 8; h += 4) {
+        b[h + 0] = c_add(a[h + 0], a[h + 2]);
+        b[h + 2] = c_sub(a[h + 0], a[h + 2]);
+        b[h + 1] = c_add(a[h + 1], a[h + 3]);
+        b[h + 3] = c_sub(a[h + 1], a[h + 3]);
+        b[h + 3] = INV ? c_mul_pi(b[h + 3]) : c_mul_mi(b[h + 3]);
+    }
+    // span-1 butterflies; results land bit-reversed: X[k] = c[bitrev3(k)]
+    double2 c[8];
+#pragma unroll
+    for (int h = 0; h < 8; h += 2) {
+        c[h] = c_add(b[h], b[h + 1]);
+        c[h + 1] = c_sub(b[h], b[h + 1]);
+    }
+    v[0] = c[0]; v[1] = c[4]; v[2] = c[2]; v[3] = c[6];
+    v[4] = c[1]; v[5] = c[5]; v[6] = c[3]; v[7] = c[7];
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(double2 (&v)[R]) {
+    if constexpr (R == 8) dft8<INV>(v);
+    else if constexpr (R == 4) dft4<INV>(v);
+    else dft2<INV>(v[0], v[1]);
+}
+
+// ----------------------------------------------------------------------------
+// superstages on one swizzled polynomial in shared memory
+//
+// forward (DIF) superstage at radix R, span S, butterfly b in [0, H/R):
+//   n1 = b % S, base = (b / S) R S + n1, inputs x[base + S n2],
+//   y = DFT_R(x), y[k2] *= W_{RS}^{n1 k2}, output y[k2] -> base + S k2.
+// inverse (DIT) superstage undoes it with conjugate twiddles (times R).
+// tw: per-stage table, row k2-1 of length S holds W_{RS}^{n1 k2}.
+// ----------------------------------------------------------------------------
+template <int R, int S, bool INV>
+__device__ __forceinline__ void twiddle(double2 (&v)[R], const double2* tw, int n1) {
+    if constexpr (S > 1) {
+#pragma unroll
+        for (int k2 = 1; k2 < R; ++k2) {
+            const double2 w = tw[(k2 - 1) * S + n1];
+            v[k2] = c_mul(v[k2], INV ? c_conj(w) : w);
+        }
+    }
+}
+
+template <int R, int S>
+__device__ __forceinline__ void dif_stage(double2* poly, const double2* tw, int b) {
+    const int n1 = b % S;
+    const int base = (b / S) * R * S + n1;
+    double2 v[R];
+#pragma unroll
+    for (int n2 = 0; n2 < R; ++n2) v[n2] = poly[swz(base + S * n2)];
+    dft<R, false>(v);
+    twiddle<R, S, false>(v, tw, n1);
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) poly[swz(base + S * k2)] = v[k2];
+}
+
+template <int R, int S>
+__device__ __forceinline__ void dit_stage(double2* poly, const double2* tw, int b) {
+    const int n1 = b % S;
+    const int base = (b / S) * R * S + n1;
+    double2 v[R];
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) v[k2] = poly[swz(base + S * k2)];
+    twiddle<R, S, true>(v, tw, n1);
+    dft<R, true>(v);
+#pragma unroll
+    for (int n2 = 0; n2 < R; ++n2) poly[swz(base + S * n2)] = v[n2];
+}
+
+// superstage s over `npoly` consecutive polynomials, spread over the CTA
+template <int LOGH, int s, bool INV>
+__device__ __forceinline__ void stage_all(double2* polys, int npoly, const double2* tw_all, int tid, int nt) {
+    using P = Plan<LOGH>;
+    constexpr int R = P::radix(s);
+    constexpr int S = P::span(s);
+    constexpr int PER = P::H / R;
+    const double2* tw = tw_all + P::tw_offset(s);
+    const int total = npoly * PER;
+    for (int t = tid; t < total; t += nt) {
+        double2* poly = polys + (t / PER) * P::H;
+        if (INV) dit_stage<R, S>(poly, tw, t % PER);
+        else dif_stage<R, S>(poly, tw, t % PER);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// device-resident FFT plan for one degree (built once per device and N)
+// ----------------------------------------------------------------------------
+struct FftPlan {
+    int N = 0;
+    double2* qt = nullptr;     // N/2: exp(-i pi r / N)
+    double2* tw = nullptr;     // Plan<LOGH>::TW per-stage twiddles
+    uint16_t* freq = nullptr;  // H: frequency of each position
+    int tw_count = 0;
+};
+
+// returns nullptr (and sets the error) when the table cannot be built
+const FftPlan* get_plan(int N);
+
+// host helpers used by the launchers
+int plan_tw_count(int logh);
+size_t br_table_bytes(int N);
+
+}  // namespace tfhe

@@ -1,0 +1,81 @@
+"""ctypes binding of libtfhe_b200.so (the C ABI declared in
+include/tfhe_b200.h).  The library is built in-tree by
+``blind-spiking-lstm_b200/build.py``; there is no fallback when it is
+missing: every entry point raises."""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtfhe_b200.so")
+
+STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "INTERNAL", 3: "OUT_OF_MEMORY", 4: "NO_DEVICE"}
+
+
+class TFHEError(RuntimeError):
+    """A non-zero status from the C ABI, with tfhe_last_error()'s message."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.status_name = STATUS.get(status, str(status))
+        super().__init__(f"{self.status_name}: {message}")
+
+
+class TfheParams(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_int32) for name in
+                ("N", "n", "n_big", "log2_beta_bs", "l_bs", "collapse", "log2_beta_ks", "l_ks", "log2_q")]
+
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+
+# name -> (restype, argtypes); every function declared in include/tfhe_b200.h
+SIGNATURES = {
+    "tfhe_version": (ctypes.c_char_p, []),
+    "tfhe_last_error": (ctypes.c_char_p, []),
+    "tfhe_mul_bootstrap": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P, _I64, _P, _I64, _I64, _I64, _I64, _P, _I64]),
+    "tfhe_keys_create": (ctypes.c_int, [ctypes.POINTER(TfheParams), _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "tfhe_keys_create_fourier": (ctypes.c_int, [ctypes.POINTER(TfheParams), _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "tfhe_keys_destroy": (None, [_P]),
+    "tfhe_keys_device_bytes": (_I64, [_P]),
+    "tfhe_keyswitch": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P]),
+    "tfhe_blind_rotate": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _I64, _P]),
+    "tfhe_sample_extract": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I64, _P]),
+    "tfhe_pbs": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _P]),
+    "tfhe_keyswitch_ref": (ctypes.c_int, [_P, _P, _P, _P, _I32, _I32, _I32, _I32, _P, _P, _I64, _P]),
+    "tfhe_rotate_extract_i64": (ctypes.c_int, [_P, _P, _I32, _I32, _I64, _P, _P, _P, _I64, _P]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library once; raise if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python blind-spiking-lstm_b200/build.py` "
+                    "(the engine has no CPU fallback)")
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = load().tfhe_last_error()
+        raise TFHEError(int(status), msg.decode() if msg else "")
+
+
+def version() -> str:
+    return load().tfhe_version().decode()

@@ -1,0 +1,179 @@
+"""Native engine: device-resident keys and batched PBS stages on torch CUDA
+tensors.  Torus values are uint32 bit patterns held in torch.int32 tensors
+(the reference's centred float64 values reduced modulo 2^32).  torch is used
+for device memory and streams only; all arithmetic runs in libtfhe_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .params import ParamSet
+
+
+def _ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+def _stream(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def _need(t, dtype, shape, name):
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch tensor")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must live on a CUDA device")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} must have shape {tuple(shape)}, got {tuple(t.shape)}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+# ---------------------------------------------------------------- torus views
+def to_u32(x) -> np.ndarray:
+    """Centred integers (float64/int64, any range) -> uint32 modulo 2^32."""
+    a = np.asarray(x)
+    if a.dtype.kind == "f":
+        a = np.rint(a)
+    return (a.astype(np.int64) & 0xFFFFFFFF).astype(np.uint32)
+
+
+def u32_as_i32(x: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint32)).view(np.int32)
+
+
+def centred(x) -> np.ndarray:
+    """uint32 / int32 bit patterns -> centred int64 in [-2^31, 2^31)."""
+    a = np.asarray(x)
+    return a.astype(np.uint32).view(np.int32).astype(np.int64)
+
+
+def device_u32(x, device=None) -> torch.Tensor:
+    """Host torus values -> int32 CUDA tensor of uint32 bit patterns."""
+    return torch.from_numpy(u32_as_i32(to_u32(x))).to(device or "cuda")
+
+
+# ---------------------------------------------------------------- keys
+class Keys:
+    """Device-resident bootstrapping and key-switching keys (tfhe_keys)."""
+
+    def __init__(self, params: ParamSet, handle: int, device: int):
+        self.params = params
+        self._h = ctypes.c_void_p(handle)
+        self.device = device
+
+    @classmethod
+    def create(cls, params: ParamSet, bsk_coeff, ksk_a, ksk_b, stream=None) -> "Keys":
+        """From the coefficient-domain key (2, 2, G*M, l_bs, N) and the
+        key-switching key (l_ks, n_big, n) / (l_ks, n_big), host arrays of
+        torus values (centred floats or unsigned)."""
+        lib = _lib.load()
+        p = params
+        bsk = np.ascontiguousarray(to_u32(bsk_coeff).reshape(2, 2, p.G * p.M, p.l_bs, p.N))
+        ka = np.ascontiguousarray(to_u32(ksk_a).reshape(p.l_ks, p.big, p.n))
+        kb = np.ascontiguousarray(to_u32(ksk_b).reshape(p.l_ks, p.big))
+        cp = p.ctypes()
+        out = ctypes.c_void_p()
+        _lib.check(lib.tfhe_keys_create(ctypes.byref(cp), bsk.ctypes.data, ka.ctypes.data, kb.ctypes.data,
+                                        _stream(stream), ctypes.byref(out)))
+        return cls(params, out.value, torch.cuda.current_device())
+
+    @classmethod
+    def create_fourier(cls, params: ParamSet, bsk_ordered, ksk_a, ksk_b, stream=None) -> "Keys":
+        """From the reference's Fourier key ``bsk_ordered`` (complex128
+        (2, 2, l_bs, G*M, N/2), nn_tfhe/activation.py:49-53)."""
+        lib = _lib.load()
+        p = params
+        bo = np.ascontiguousarray(np.asarray(bsk_ordered, dtype=np.complex128)
+                                  .reshape(2, 2, p.l_bs, p.G * p.M, p.N // 2))
+        ka = np.ascontiguousarray(to_u32(ksk_a).reshape(p.l_ks, p.big, p.n))
+        kb = np.ascontiguousarray(to_u32(ksk_b).reshape(p.l_ks, p.big))
+        cp = p.ctypes()
+        out = ctypes.c_void_p()
+        _lib.check(lib.tfhe_keys_create_fourier(ctypes.byref(cp), bo.ctypes.data, ka.ctypes.data,
+                                                kb.ctypes.data, _stream(stream), ctypes.byref(out)))
+        return cls(params, out.value, torch.cuda.current_device())
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if not self._h or not self._h.value:
+            raise RuntimeError("keys have been released")
+        return self._h
+
+    def device_bytes(self) -> int:
+        return int(_lib.load().tfhe_keys_device_bytes(self.handle))
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            _lib.load().tfhe_keys_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ stages
+    def keyswitch(self, a, b, a_out=None, b_out=None, stream=None):
+        """key_switch_LWE over a batch: a (B, n_big), b (B) -> (B, n), (B)."""
+        p = self.params
+        B = a.shape[0]
+        _need(a, torch.int32, (B, p.big), "a")
+        _need(b, torch.int32, (B,), "b")
+        a_out = a_out if a_out is not None else torch.empty((B, p.n), dtype=torch.int32, device=a.device)
+        b_out = b_out if b_out is not None else torch.empty((B,), dtype=torch.int32, device=a.device)
+        _need(a_out, torch.int32, (B, p.n), "a_out")
+        _need(b_out, torch.int32, (B,), "b_out")
+        _lib.check(_lib.load().tfhe_keyswitch(self.handle, _ptr(a), _ptr(b), _ptr(a_out), _ptr(b_out), B,
+                                              _stream(stream)))
+        return a_out, b_out
+
+    def blind_rotate(self, lwe_a, lwe_b, lut, n_lut=1, acc_out=None, stream=None):
+        """BR: lwe (B, n) / (B), lut (1|B, 2, N) -> ACC (B, 2, N)."""
+        p = self.params
+        B = lwe_a.shape[0]
+        _need(lwe_a, torch.int32, (B, p.n), "lwe_a")
+        _need(lwe_b, torch.int32, (B,), "lwe_b")
+        _need(lut, torch.int32, (lut.shape[0], 2, p.N), "lut")
+        acc_out = acc_out if acc_out is not None else torch.empty((B, 2, p.N), dtype=torch.int32,
+                                                                  device=lwe_a.device)
+        _need(acc_out, torch.int32, (B, 2, p.N), "acc_out")
+        _lib.check(_lib.load().tfhe_blind_rotate(self.handle, _ptr(lwe_a), _ptr(lwe_b), _ptr(lut), lut.shape[0],
+                                                 n_lut, _ptr(acc_out), B, _stream(stream)))
+        return acc_out
+
+    def pbs(self, a, b, lut, n_lut=1, out_a=None, out_b=None, stream=None):
+        """Key switch + blind rotation + many-LUT extraction
+        (HeavysideBoostrapper.cuboot): a (B, n_big), b (B), lut (1|B, 2, N)
+        -> out_a (B, n_lut, N), out_b (B, n_lut)."""
+        p = self.params
+        B = a.shape[0]
+        _need(a, torch.int32, (B, p.big), "a")
+        _need(b, torch.int32, (B,), "b")
+        _need(lut, torch.int32, (lut.shape[0], 2, p.N), "lut")
+        out_a = out_a if out_a is not None else torch.empty((B, n_lut, p.N), dtype=torch.int32, device=a.device)
+        out_b = out_b if out_b is not None else torch.empty((B, n_lut), dtype=torch.int32, device=a.device)
+        _need(out_a, torch.int32, (B, n_lut, p.N), "out_a")
+        _need(out_b, torch.int32, (B, n_lut), "out_b")
+        _lib.check(_lib.load().tfhe_pbs(self.handle, _ptr(a), _ptr(b), _ptr(lut), lut.shape[0], n_lut,
+                                        _ptr(out_a), _ptr(out_b), B, _stream(stream)))
+        return out_a, out_b
+
+
+def sample_extract(acc, n_lut=1, out_a=None, out_b=None, stream=None):
+    """Many-LUT sample extraction: acc (B, 2, N) -> (B, n_lut, N), (B, n_lut)."""
+    B, two, N = acc.shape
+    _need(acc, torch.int32, (B, 2, N), "acc")
+    out_a = out_a if out_a is not None else torch.empty((B, n_lut, N), dtype=torch.int32, device=acc.device)
+    out_b = out_b if out_b is not None else torch.empty((B, n_lut), dtype=torch.int32, device=acc.device)
+    _lib.check(_lib.load().tfhe_sample_extract(_ptr(acc), N, n_lut, _ptr(out_a), _ptr(out_b), B,
+                                               _stream(stream)))
+    return out_a, out_b

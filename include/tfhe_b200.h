@@ -1,0 +1,160 @@
+/*
+ * tfhe_b200.h - C ABI of the B200 (sm_100a) TFHE programmable-bootstrapping
+ * engine: LWE key switching, collapsed blind rotation and many-LUT sample
+ * extraction for the encrypted Spike-LSTM of AMIAD-Research/Blind-Spiking-LSTM.
+ *
+ * Conventions
+ *  - Every compute entry point takes DEVICE pointers, runs asynchronously on
+ *    the given CUDA stream (cudaStream_t passed as void*, NULL = legacy
+ *    default stream) and returns a status code (TFHE_OK = 0).  The message
+ *    of the last failing call on the calling thread is tfhe_last_error().
+ *  - Native entry points carry torus values as uint32 (q = 2^32), the
+ *    reference's float64 values centred in [-q/2, q/2] reduced modulo 2^32.
+ *  - tfhe_mul_bootstrap keeps the reference's int64 / complex128 buffers.
+ *  - No torch, JAX or C++ types cross this boundary.
+ */
+#ifndef TFHE_B200_H
+#define TFHE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TFHE_B200_ABI_VERSION 1
+
+/* status codes: the reference handler returns ffi::Error::InvalidArgument
+ * for unsupported degree / l and ffi::Error::Internal for launch failures
+ * (csrc/mul_bootstrap.cuh:183-188, 211-223). */
+enum {
+    TFHE_OK = 0,
+    TFHE_ERR_INVALID_ARGUMENT = 1,
+    TFHE_ERR_INTERNAL = 2,
+    TFHE_ERR_OUT_OF_MEMORY = 3,
+    TFHE_ERR_NO_DEVICE = 4
+};
+
+/* Parameter set of one bootstrapping key (the reference keeps these in the
+ * dict_params* globals of parameters_crypto.py:6-84). */
+typedef struct tfhe_params {
+    int32_t N;             /* GLWE degree: 128 .. 4096, power of two            */
+    int32_t n;             /* LWE dimension of the blind rotation               */
+    int32_t n_big;         /* LWE dimension entering the key switch (usually N) */
+    int32_t log2_beta_bs;  /* blind-rotation gadget base, log2                  */
+    int32_t l_bs;          /* blind-rotation gadget levels: 1 .. 4              */
+    int32_t collapse;      /* collapse factor c (n % c == 0): 1 .. 4            */
+    int32_t log2_beta_ks;  /* key-switch gadget base, log2                      */
+    int32_t l_ks;          /* key-switch gadget levels: 1 .. 8                  */
+    int32_t log2_q;        /* must be 32 for the native entry points            */
+} tfhe_params;
+
+typedef struct tfhe_keys tfhe_keys;   /* device-resident key material */
+
+/* library identification and the last error of the calling thread */
+const char* tfhe_version(void);
+const char* tfhe_last_error(void);
+
+/*
+ * Drop-in for the reference's XLA FFI handler "mul_bootstrap"
+ * (csrc/mul_bootstrap.cuh:192-243, registered at cuTFHE/multiply.py:10-14,
+ * called at cuTFHE/multiply.py:17-51): the collapsed CMux chain
+ * (multiply_seq_monomial's kernel) on reference-layout buffers.
+ *   ct_init      int64 (..., 2, N); ct_elems == 2N broadcasts one ACC
+ *                (batch stride 0, mul_bootstrap.cuh:162-164)
+ *   bsk          complex128, last six dims (G, 2, L, 2, M, N/2)
+ *                (multiply.py:81-86); bsk_dims = those six extents
+ *   all_rot_fft  complex128 (2N, N/2): row r = jax_fourier(X^r)
+ *   indices      int32 (batch, G, M)
+ *   out          int64 (batch, 2, N)
+ * degree in {128..4096}, l in {1..4}; other values -> INVALID_ARGUMENT.
+ * log2_q: 2..64 with the reference's float64 semantics (exact for <= 53).
+ */
+int tfhe_mul_bootstrap(void* stream,
+                       const int64_t* ct_init, int64_t ct_elems,
+                       const void* bsk, const int64_t* bsk_dims,
+                       const void* all_rot_fft, int64_t all_rot_rows,
+                       const int32_t* indices,
+                       int64_t log2_beta, int64_t log2_q, int64_t l, int64_t degree,
+                       int64_t* out, int64_t batch);
+
+/*
+ * Upload key material (HOST pointers) and convert it to the device layout;
+ * returns after the upload has finished.  Replaces the key arrays the
+ * reference passes into every call (HeavysideBoostrapper's
+ * bootstrapping_key / key_switching_key_bs, nn_tfhe/activation.py:88-97).
+ *   bsk_coeff  uint32 (2 left/right, 2 mask/body, G*M, l_bs, N): the
+ *              coefficient-domain key of get_boostrapping_key_collapse
+ *              (schemas/RLWE_jax.py:162-197) modulo 2^32
+ *   ksk_a      uint32 (l_ks, n_big, n), ksk_b uint32 (l_ks, n_big): the key
+ *              of get_keyswitch_sk_LWE (schemas/LWE_jax.py:86-93)
+ */
+int tfhe_keys_create(const tfhe_params* params, const uint32_t* bsk_coeff,
+                     const uint32_t* ksk_a, const uint32_t* ksk_b,
+                     void* stream, tfhe_keys** keys_out);
+
+/* Same, from the reference's Fourier key ``bsk_ordered`` (complex128
+ * (2, 2, l_bs, G*M, N/2), nn_tfhe/activation.py:49-53) as interleaved
+ * doubles. */
+int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordered,
+                             const uint32_t* ksk_a, const uint32_t* ksk_b,
+                             void* stream, tfhe_keys** keys_out);
+
+void tfhe_keys_destroy(tfhe_keys* keys);
+int64_t tfhe_keys_device_bytes(const tfhe_keys* keys);
+
+/* Batched LWE key switch: key_switch_LWE vmapped over ciphertexts
+ * (schemas/LWE_jax.py:97-117 as called at nn_tfhe/activation.py:150).
+ * a_in (batch, n_big), b_in (batch) -> a_out (batch, n), b_out (batch). */
+int tfhe_keyswitch(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in,
+                   uint32_t* a_out, uint32_t* b_out, int64_t batch, void* stream);
+
+/* Blind rotation then rotation by -b~: BR (schemas/RLWE_jax.py:305-315).
+ * lwe_a (batch, n), lwe_b (batch): key-switched LWEs; lut (lut_count, 2, N)
+ * with lut_count == 1 (shared) or == batch; acc_out (batch, 2, N). */
+int tfhe_blind_rotate(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b,
+                      const uint32_t* lut, int64_t lut_count, int32_t n_lut,
+                      uint32_t* acc_out, int64_t batch, void* stream);
+
+/* Many-LUT sample extraction at alpha = 0 .. n_lut-1
+ * (schemas/text_jax.py:191-208 vmapped as in schemas/RLWE_jax.py:301-303).
+ * acc (batch, 2, N) -> out_a (batch, n_lut, N), out_b (batch, n_lut). */
+int tfhe_sample_extract(const uint32_t* acc, int32_t N, int32_t n_lut,
+                        uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
+
+/* Full programmable bootstrap: key switch, blind rotation, rotation by -b~
+ * and many-LUT extraction, HeavysideBoostrapper.cuboot
+ * (nn_tfhe/activation.py:148-162) = cuboot_merge(key_switch_LWE(h)).
+ * a_in (batch, n_big), b_in (batch), lut (lut_count, 2, N)
+ * -> out_a (batch, n_lut, N), out_b (batch, n_lut).
+ * The key-switched intermediate is allocated stream-ordered on `stream`. */
+int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in,
+             const uint32_t* lut, int64_t lut_count, int32_t n_lut,
+             uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
+
+/* key_switch_LWE (schemas/LWE_jax.py:97-117) with the key in the
+ * reference's own layout, as DEVICE uint32 arrays: ksk_a (l_ks, n_big, n)
+ * and ksk_b (l_ks, n_big) (the pk / b of get_keyswitch_sk_LWE modulo 2^32).
+ * a_in (batch, n_big), b_in (batch) -> a_out (batch, n), b_out (batch). */
+int tfhe_keyswitch_ref(const uint32_t* a_in, const uint32_t* b_in,
+                       const uint32_t* ksk_a, const uint32_t* ksk_b,
+                       int32_t n_big, int32_t n, int32_t l_ks, int32_t log2_beta_ks,
+                       uint32_t* a_out, uint32_t* b_out, int64_t batch, void* stream);
+
+/* The steps of cuboot_merge / BR after the kernel (schemas/RLWE_jax.py:
+ * 295-303 and 305-315) on the reference's int64 values, keeping its
+ * +-q/2 representatives: b~ = round(2N b / (q n_lut)) n_lut, ACC rotated by
+ * X^(-b~), then sample_extract at alpha = 0 .. n_lut-1.
+ *   acc (batch, 2, N) int64 (tfhe_mul_bootstrap's output), b (batch) float64
+ *   out_acc (batch, 2, N) and/or out_a (batch, n_lut, N) + out_b
+ *   (batch, n_lut), all int64; pass NULL for outputs not wanted. */
+int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int32_t n_lut,
+                            int64_t log2_q, int64_t* out_acc, int64_t* out_a, int64_t* out_b,
+                            int64_t batch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TFHE_B200_H */

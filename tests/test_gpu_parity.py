@@ -1,0 +1,300 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Integer stages (key switching, digits, rotation indices, rotations,
+extraction) must be bit-exact.  The FP64 external product is bit-exact
+against the oracle whenever its rounding error stays below 1/2 (beta <= 2^7
+here: measured max error 0.03); with beta = 2^15 it is compared with the
+exact integer product within a stated bound, and by decryption."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import tfhe_oracle as O
+from pbs_cases import PARAMS, canon, inputs, keys, ks_params, many_lut_body, step_body
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover - CPU runs deselect -m gpu
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from tfhe_b200 import TFHEError, ops  # noqa: E402
+from tfhe_b200.engine import Keys, centred, device_u32, sample_extract  # noqa: E402
+from tfhe_b200.params import ParamSet  # noqa: E402
+
+# FFT rounding bound used where the FP64 product is not exact (beta = 2^15):
+# |engine - exact| <= FFT_TOL units of q/2^32 per coefficient
+FFT_TOL = 64
+
+
+def pset(name):
+    p = PARAMS[name]
+    lg = lambda v: int(round(np.log2(v)))
+    return ParamSet(name, N=p["N"], n=p["n"], log2_beta_bs=lg(p["beta_bs"]), l_bs=p["l_bs"],
+                    collapse=p["collapse"], log2_beta_ks=lg(p["beta_ks"]), l_ks=p["l_ks"],
+                    sigma_glwe=p["sigma_glwe"], sigma_lwe=p["sigma_lwe"])
+
+
+_ENG = {}
+
+
+def engine(name):
+    if name not in _ENG:
+        k = keys(name)
+        _ENG[name] = Keys.create(pset(name), k.bsk_coeff, k.ksk[0], k.ksk[1].reshape(k.ksk[1].shape[:2]))
+    return _ENG[name]
+
+
+def u32(x):
+    return (np.rint(np.asarray(x, dtype=np.float64)).astype(np.int64) & 0xFFFFFFFF).astype(np.uint32)
+
+
+def host_u32(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+def torus_dist(a, b):
+    """|a - b| on Z/2^32 (elementwise, as int64)"""
+    d = (u32(a).astype(np.int64) - u32(b).astype(np.int64)) & 0xFFFFFFFF
+    return np.minimum(d, 2 ** 32 - d)
+
+
+@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2"])
+def test_keyswitch_bit_exact(name):
+    k = keys(name)
+    msgs, a, b = inputs(name, 37)
+    ra, rb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+    ea, eb = engine(name).keyswitch(device_u32(a), device_u32(b.reshape(-1)))
+    assert np.array_equal(host_u32(ea), u32(ra))
+    assert np.array_equal(host_u32(eb), u32(rb.reshape(-1)))
+
+
+@pytest.mark.parametrize("name,batch,n_lut", [("tiny_c3", 9, 1), ("tiny_c3", 5, 4), ("cfg1", 6, 1),
+                                              ("cfg1", 5, 4)])
+def test_blind_rotate_bit_exact(name, batch, n_lut):
+    """BR (schemas/RLWE_jax.py:305-315) at beta = 2^7: bit-exact."""
+    p = PARAMS[name]
+    k = keys(name)
+    msgs, a, b = inputs(name, batch)
+    ca, cb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+    body = step_body(name) if n_lut == 1 else many_lut_body(name, n_lut)
+    enc = [np.zeros((batch, p["N"])), np.broadcast_to(body, (batch, p["N"]))]
+    want = O.BR((ca, cb), enc, k.bsk_ordered, p["q"], p["beta_bs"], p["l_bs"], p["N"], p["collapse"],
+                k.all_rot, n_lut)
+    lut = device_u32(np.stack([np.zeros(p["N"]), body])[None])
+    acc = engine(name).blind_rotate(device_u32(ca), device_u32(cb.reshape(-1)), lut, n_lut=n_lut)
+    assert np.array_equal(host_u32(acc), u32(want))
+
+
+@pytest.mark.parametrize("name,batch", [("tiny_c3", 7), ("cfg1", 12)])
+def test_pbs_bit_exact_and_decrypts(name, batch):
+    """tfhe_pbs = cuboot_merge(key_switch_LWE(h)) (activation.py:148-162)."""
+    p = PARAMS[name]
+    k = keys(name)
+    msgs, a, b = inputs(name, batch)
+    ca, cb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+    body = step_body(name)
+    enc = [np.zeros((batch, p["N"])), np.broadcast_to(body, (batch, p["N"]))]
+    wa, wb = O.cuboot_merge((ca, cb), enc, k.bsk_ordered, p["q"], p["beta_bs"], p["l_bs"], p["N"],
+                            p["collapse"], k.all_rot, 1)
+    lut = device_u32(np.stack([np.zeros(p["N"]), body])[None])
+    oa, ob = engine(name).pbs(device_u32(a), device_u32(b.reshape(-1)), lut, n_lut=1)
+    assert np.array_equal(host_u32(oa), u32(wa))
+    assert np.array_equal(host_u32(ob), u32(wb[..., 0]))
+    dec = O.decrypt_LWE((centred(host_u32(oa)[:, 0]), centred(host_u32(ob)[:, 0])), k.sk_glwe,
+                        {"t": 32, "q": p["q"]})
+    want = O.decrypt_LWE((wa[:, 0], wb[:, 0]), k.sk_glwe, {"t": 32, "q": p["q"]})
+    assert np.array_equal(dec, want)
+
+
+def test_pbs_per_ciphertext_luts_and_ragged_batches():
+    """lut_count == batch, batch sizes around the CTA width, batch 1 and 0."""
+    name = "tiny_c3"
+    p = PARAMS[name]
+    k = keys(name)
+    eng = engine(name)
+    rng = np.random.default_rng(7)
+    for batch in (1, 2, 15, 16, 17, 33):
+        msgs, a, b = inputs(name, batch, seed_offset=batch)
+        bodies = canon(rng.integers(-2 ** 31, 2 ** 31, size=(batch, p["N"])))
+        masks = canon(rng.integers(-2 ** 31, 2 ** 31, size=(batch, p["N"])))
+        ca, cb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+        wa, wb = O.cuboot_merge((ca, cb), [masks, bodies], k.bsk_ordered, p["q"], p["beta_bs"], p["l_bs"],
+                                p["N"], p["collapse"], k.all_rot, 2)
+        lut = device_u32(np.stack([masks, bodies], axis=1))
+        oa, ob = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut, n_lut=2)
+        assert np.array_equal(host_u32(oa), u32(wa)), batch
+        assert np.array_equal(host_u32(ob), u32(wb[..., 0])), batch
+    empty = torch.empty((0, p["N"]), dtype=torch.int32, device="cuda")
+    oa, ob = eng.pbs(empty, torch.empty((0,), dtype=torch.int32, device="cuda"),
+                     device_u32(np.zeros((1, 2, p["N"]))), n_lut=1)
+    assert oa.shape == (0, 1, p["N"]) and ob.shape == (0, 1)
+
+
+@pytest.mark.parametrize("name,batch", [("tiny_c2", 6), ("cfg2", 3)])
+def test_beta15_against_exact_product(name, batch):
+    """beta = 2^15: the FP64 product is not exact; compare with the exact
+    integer chain and with the decryptions."""
+    p = PARAMS[name]
+    k = keys(name)
+    msgs, a, b = inputs(name, batch, t=16)
+    ca, cb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+    body = step_body(name, t=16)
+    enc = [np.zeros((batch, p["N"])), np.broadcast_to(body, (batch, p["N"]))]
+    exact = O.BR((ca, cb), enc, k.bsk_ordered, p["q"], p["beta_bs"], p["l_bs"], p["N"], p["collapse"],
+                 k.all_rot, 1, exact_bsk=k.bsk_coeff)
+    lut = device_u32(np.stack([np.zeros(p["N"]), body])[None])
+    acc = host_u32(engine(name).blind_rotate(device_u32(ca), device_u32(cb.reshape(-1)), lut))
+    # a single-group error feeds later digits, so compare phases: decrypt
+    # the extracted LWEs of both and compare messages and noise
+    ea, eb = O.extract_many(centred(acc).astype(np.float64), 1)
+    xa, xb = O.extract_many(exact, 1)
+    sk = k.sk_glwe
+    dec_e = O.decrypt_LWE((ea[:, 0], eb[:, 0]), sk, {"t": 16, "q": p["q"]})
+    dec_x = O.decrypt_LWE((xa[:, 0], xb[:, 0]), sk, {"t": 16, "q": p["q"]})
+    assert np.array_equal(dec_e, dec_x)
+    assert np.array_equal(dec_x, (msgs >= 4).astype(float))
+
+
+@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "c1_N128", "c4_N4096", "cfg1"])
+def test_one_group_against_exact(name):
+    """One CMux group through tfhe_mul_bootstrap (reference layout) against
+    the exact integer product: max error bounded, bit-exact when beta <= 2^8."""
+    p = PARAMS[name]
+    k = keys(name)
+    c = p["collapse"]
+    batch = 4
+    rng = np.random.default_rng(99)
+    acc0 = canon(rng.integers(-2 ** 31, 2 ** 31, size=(batch, 2, p["N"])))
+    pk = canon(rng.integers(-2 ** 31, 2 ** 31, size=(batch, c)))
+    # keys restricted to the first group
+    G = p["n"] // c
+    M = 2 ** c
+    bsk1 = k.bsk_ordered.reshape(2, 2, p["l_bs"], G, M, p["N"] // 2)[:, :, :, :1].reshape(
+        2, 2, p["l_bs"], M, p["N"] // 2)
+    coeff1 = k.bsk_coeff.reshape(2, 2, G, M, p["l_bs"], p["N"])[:, :, :1].reshape(2, 2, M, p["l_bs"], p["N"])
+    exact = O.multiply_seq_monomial_exact(acc0, pk, coeff1, p["q"], p["beta_bs"], p["l_bs"], p["N"], c, 1)
+    got = ops.multiply_seq_monomial(torch.from_numpy(acc0).cuda(), torch.from_numpy(pk).cuda(),
+                                    torch.from_numpy(bsk1).cuda(), 32, int(np.log2(p["beta_bs"])), p["l_bs"],
+                                    p["N"], c, torch.from_numpy(k.all_rot).cuda(), 1).cpu().numpy()
+    err = torus_dist(got, exact)
+    if p["beta_bs"] <= 2 ** 8:
+        assert err.max() == 0
+        assert np.array_equal(got, exact)          # incl. the +-q/2 representative
+    assert err.max() <= FFT_TOL, err.max()
+
+
+@pytest.mark.parametrize("name,batch", [("tiny_c3", 5), ("cfg1", 3)])
+def test_mul_bootstrap_dropin_matches_reference_path(name, batch):
+    """tfhe_mul_bootstrap on reference buffers == multiply_seq_monomial of
+    the oracle (float64 values, +-q/2 representatives included)."""
+    p = PARAMS[name]
+    k = keys(name)
+    msgs, a, b = inputs(name, batch)
+    ca, cb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+    body = step_body(name)
+    ct = np.stack([np.zeros((batch, p["N"])), np.broadcast_to(body, (batch, p["N"]))], axis=1)
+    want = O.multiply_seq_monomial(ct, ca, k.bsk_ordered, p["q"], p["beta_bs"], p["l_bs"], p["N"],
+                                   p["collapse"], k.all_rot, 1)
+    got = ops.multiply_seq_monomial(torch.from_numpy(ct).cuda(), torch.from_numpy(ca).cuda(),
+                                    torch.from_numpy(k.bsk_ordered).cuda(), 32, int(np.log2(p["beta_bs"])),
+                                    p["l_bs"], p["N"], p["collapse"], torch.from_numpy(k.all_rot).cuda(), 1)
+    assert np.array_equal(got.cpu().numpy(), want)
+    # broadcast ACC (ct_init of 2N elements, stride 0)
+    got1 = ops.multiply_seq_monomial(torch.from_numpy(ct[:1]).cuda(), torch.from_numpy(ca).cuda(),
+                                     torch.from_numpy(k.bsk_ordered).cuda(), 32, int(np.log2(p["beta_bs"])),
+                                     p["l_bs"], p["N"], p["collapse"], torch.from_numpy(k.all_rot).cuda(), 1)
+    assert np.array_equal(got1.cpu().numpy(), want)
+
+
+def test_fourier_key_upload_equals_coefficient_upload():
+    name = "tiny_c3"
+    k = keys(name)
+    e2 = Keys.create_fourier(pset(name), k.bsk_ordered, k.ksk[0], k.ksk[1].reshape(k.ksk[1].shape[:2]))
+    msgs, a, b = inputs(name, 8)
+    lut = device_u32(np.stack([np.zeros(PARAMS[name]["N"]), step_body(name)])[None])
+    o1 = engine(name).pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+    o2 = e2.pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+    assert torch.equal(o1[0], o2[0]) and torch.equal(o1[1], o2[1])
+    e2.close()
+
+
+def test_standalone_extract_and_rotate_ops():
+    rng = np.random.default_rng(5)
+    N = 256
+    acc = canon(rng.integers(-2 ** 31, 2 ** 31, size=(3, 2, N)))
+    oa, ob = sample_extract(device_u32(acc), n_lut=5)
+    wa, wb = O.extract_many(acc, 5)
+    assert np.array_equal(host_u32(oa), u32(wa)) and np.array_equal(host_u32(ob), u32(wb[..., 0]))
+    for alpha in (0, 1, 100, 255):
+        ga, gb = ops.sample_extract((torch.from_numpy(acc[0, 0]).cuda(), torch.from_numpy(acc[0, 1]).cuda()), alpha)
+        ra, rb = O.sample_extract((acc[0, 0], acc[0, 1]), alpha)
+        assert np.array_equal(ga.cpu().numpy(), ra) and np.array_equal(gb.cpu().numpy(), rb)
+    for e in (0, 1, -1, 255, 256, 257, -256, -300, 511, 512, 700, -700):
+        ga, gb = ops.rotate_ciphertext((torch.from_numpy(acc[1, 0]).cuda(), torch.from_numpy(acc[1, 1]).cuda()), e)
+        ra, rb = O.rotate_ciphertext((acc[1, 0], acc[1, 1]), e)
+        assert np.array_equal(ga.cpu().numpy(), ra) and np.array_equal(gb.cpu().numpy(), rb), e
+
+
+def test_repeat_runs_identical():
+    """Any run-to-run difference would flag a race on shared memory."""
+    name = "cfg1"
+    msgs, a, b = inputs(name, 9)
+    lut = device_u32(np.stack([np.zeros(PARAMS[name]["N"]), step_body(name)])[None])
+    first = engine(name).pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+    for _ in range(2):
+        again = engine(name).pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+        assert torch.equal(first[0], again[0]) and torch.equal(first[1], again[1])
+
+
+def test_invalid_arguments_raise():
+    eng = engine("tiny_c3")
+    N = PARAMS["tiny_c3"]["N"]
+    a = torch.zeros((4, N), dtype=torch.int32, device="cuda")
+    b = torch.zeros((4,), dtype=torch.int32, device="cuda")
+    lut3 = torch.zeros((3, 2, N), dtype=torch.int32, device="cuda")
+    with pytest.raises(TFHEError, match="INVALID_ARGUMENT"):
+        eng.pbs(a, b, lut3)
+    with pytest.raises(TFHEError, match="INVALID_ARGUMENT"):
+        eng.pbs(a, b, lut3[:1], n_lut=0)
+    bad = pset("tiny_c3").with_(N=300)
+    k = keys("tiny_c3")
+    with pytest.raises((TFHEError, ValueError)):
+        Keys.create(bad, k.bsk_coeff, k.ksk[0], k.ksk[1])
+
+
+@pytest.mark.parametrize("name,batch,n_lut", [("tiny_c3", 6, 1), ("tiny_c3", 6, 4), ("cfg1", 4, 1),
+                                              ("cfg1", 4, 4)])
+def test_reference_golden_fixtures(name, batch, n_lut):
+    """The engine reproduces the outputs recorded from the reference's own
+    Python code (tests/golden/make_golden.py)."""
+    import os
+    G = np.load(os.path.join(os.path.dirname(__file__), "golden", "pbs_golden.npz"))
+    p = PARAMS[name]
+    k = O.keygen(p, {"tiny_c3": 11, "cfg1": 13}[name])
+    if np.any(np.abs(k.bsk_coeff) == 2 ** 31) or np.any(np.abs(k.ksk[0]) == 2 ** 31):
+        pytest.skip("key holds +-q/2: the uint32 view changes the reference's representative")
+    ks = ParamSet(name, N=p["N"], n=p["n"], log2_beta_bs=7, l_bs=p["l_bs"], collapse=p["collapse"],
+                  log2_beta_ks=3, l_ks=p["l_ks"], sigma_glwe=p["sigma_glwe"], sigma_lwe=p["sigma_lwe"])
+    eng = Keys.create(ks, k.bsk_coeff, k.ksk[0], k.ksk[1].reshape(k.ksk[1].shape[:2]))
+    a, b = G[f"{name}_in_a"], G[f"{name}_in_b"]
+    ka, kb = eng.keyswitch(device_u32(a), device_u32(b.reshape(-1)))
+    assert np.array_equal(host_u32(ka), u32(G[f"{name}_ks_a"]))
+    assert np.array_equal(host_u32(kb), u32(G[f"{name}_ks_b"].reshape(-1)))
+    body = G[f"{name}_lut{n_lut}"]
+    lut = device_u32(np.stack([np.zeros(p["N"]), body])[None])
+    oa, ob = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut, n_lut=n_lut)
+    assert np.array_equal(host_u32(oa), u32(G[f"{name}_merge{n_lut}_a"]))
+    assert np.array_equal(host_u32(ob), u32(G[f"{name}_merge{n_lut}_b"][..., 0]))
+    # the reference-surface mirror on the reference's float64 buffers
+    ga, gb = ops.cuboot_merge((torch.from_numpy(G[f"{name}_ks_a"]).cuda(), torch.from_numpy(G[f"{name}_ks_b"]).cuda()),
+                              [torch.zeros((batch, p["N"]), dtype=torch.float64),
+                               torch.from_numpy(np.broadcast_to(body, (batch, p["N"])).copy())],
+                              torch.from_numpy(k.bsk_ordered).cuda(), p["q"], p["beta_bs"], p["l_bs"], p["N"],
+                              p["collapse"], torch.from_numpy(k.all_rot).cuda(), n_lut)
+    assert np.array_equal(ga.cpu().numpy(), G[f"{name}_merge{n_lut}_a"])
+    assert np.array_equal(gb.cpu().numpy(), G[f"{name}_merge{n_lut}_b"])
+    kk = ops.key_switch_LWE((torch.from_numpy(k.ksk[0]).cuda(), torch.from_numpy(k.ksk[1]).cuda()),
+                            (torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()), ks_params(name))
+    assert np.array_equal(u32(kk[0].cpu().numpy()), u32(G[f"{name}_ks_a"]))
+    assert np.array_equal(u32(kk[1].cpu().numpy()), u32(G[f"{name}_ks_b"]))
+    eng.close()
