@@ -1,0 +1,440 @@
+"""Benchmark of the B200 TFHE programmable-bootstrapping engine.
+
+Workload: the batched PBS + key-switch throughput case at the 2048
+parameter set (uint32 torus, n=742, N=2048, gadget 2^15 x 2, key switch
+2^4 x 5, collapse 2), 16384 ciphertexts per step (default), uniform Z_8
+messages with a padding bit, each ciphertext with its own LUT drawn from 8
+fixed random tables f: Z_8 -> Z_8.  One step = key switch + blind rotation
++ rotation + sample extraction of the whole batch.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+  python bench.py --impl reference ...   (the CPU statement of the path)
+
+Prints ONE JSON line on rank 0.  ``value`` is device-resident throughput;
+``e2e`` is the same metric through tfhe_pbs with host buffers and the
+host<->device copies inside the timed region.  Multi-GPU runs are
+independent replicas (every PBS is independent; no collective is needed).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "blind-spiking-lstm_b200"))
+
+METRIC = "PBS/s (key switch + blind rotation + many-LUT extraction) at 0 decrypt errors"
+UNIT = "PBS/s"
+T_MSG = 16           # Z_8 messages with a padding bit: phase m q / 16
+N_TABLES = 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16384)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-sample", type=int, default=96, help="ciphertexts in the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def flops_per_pbs(p):
+    """Algorithmic blind-rotation work per PBS: per group, (2L + 2) H-point
+    transforms at 5 H log2 H flops and the pointwise contraction at
+    8 H (2 * 2L * M + 2 * 2L) flops (H = N/2), times G groups."""
+    H = p.N // 2
+    per_group = (2 * p.l_bs + 2) * 5 * H * math.log2(H) + 8 * H * (2 * 2 * p.l_bs * p.M + 2 * 2 * p.l_bs)
+    return per_group * p.G
+
+
+def workload_name(p, batch):
+    return (f"PBS+KS n={p.n} N={p.N} gadget 2^{p.log2_beta_bs}x{p.l_bs} KS 2^{p.log2_beta_ks}x{p.l_ks} "
+            f"collapse {p.collapse}, batch {batch}, per-ciphertext LUT from {N_TABLES} random Z_8 tables")
+
+
+# ---------------------------------------------------------------- inputs
+def make_inputs(p, batch, seed):
+    import numpy as np
+    from tfhe_b200 import client
+    keys = client.keygen(p, seed)
+    rng = np.random.default_rng(seed + 1)
+    msgs = rng.integers(0, T_MSG // 2, size=batch)
+    a, b = client.encrypt(keys, msgs, T_MSG, rng)
+    tables = rng.integers(0, T_MSG // 2, size=(N_TABLES, T_MSG // 2))
+    which = rng.integers(0, N_TABLES, size=batch)
+    bodies = np.stack([client.table_lut(p.N, tables[i], T_MSG) for i in range(N_TABLES)])
+    lut = np.zeros((batch, 2, p.N), dtype=np.uint32)
+    lut[:, 1] = bodies[which]
+    expect = tables[which, msgs]
+    return keys, msgs, a, b, lut, expect
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv") \
+            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/tfhe_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        load = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- engine arm
+def run_engine(args, rank, world, local_rank, dist):
+    import numpy as np
+    import torch
+    from tfhe_b200 import client
+    from tfhe_b200.engine import Keys, probe_fp64_peak
+    from tfhe_b200.params import CONFIG2
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    p = CONFIG2
+    B = args.batch
+    keys, msgs, a, b, lut, expect = make_inputs(p, B, args.seed + rank)
+    eng = Keys.create(p, keys.bsk, keys.ksk_a, keys.ksk_b)
+    i32 = lambda x: torch.from_numpy(np.ascontiguousarray(x).view(np.int32))
+    a_h, b_h, lut_h = i32(a).pin_memory(), i32(b).pin_memory(), i32(lut).pin_memory()
+    a_d, b_d, lut_d = a_h.to(dev), b_h.to(dev), lut_h.to(dev)
+    ka = torch.empty((B, p.n), dtype=torch.int32, device=dev)
+    kb = torch.empty((B,), dtype=torch.int32, device=dev)
+    oa = torch.empty((B, 1, p.N), dtype=torch.int32, device=dev)
+    ob = torch.empty((B, 1), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def step_device(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        eng.keyswitch(a_d, b_d, ka, kb)
+        if ev is not None:
+            ev[1].record(stream)
+        eng.cuboot_merge(ka, kb, lut_d, 1, oa, ob)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    peak_fp64 = probe_fp64_peak()
+
+    clocks = ClockSampler(local_rank)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for s in range(args.steps):
+        step_device(evs[s])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    dev_ms = t0.elapsed_time(t1)
+    ks_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    br_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+
+    # decryption check of the device outputs
+    out_a = oa.cpu().numpy().view(np.uint32)[:, 0]
+    out_b = ob.cpu().numpy().view(np.uint32)[:, 0]
+    dec = client.decrypt(out_a, out_b, keys.sk_glwe, T_MSG)
+    errors = int(np.sum(dec != expect))
+
+    # end to end through tfhe_pbs with host buffers
+    oa_h = torch.empty((B, 1, p.N), dtype=torch.int32).pin_memory()
+    ob_h = torch.empty((B, 1), dtype=torch.int32).pin_memory()
+    a_e = torch.empty_like(a_d)
+    b_e = torch.empty_like(b_d)
+    lut_e = torch.empty_like(lut_d)
+    oa_e = torch.empty_like(oa)
+    ob_e = torch.empty_like(ob)
+
+    def step_e2e():
+        a_e.copy_(a_h, non_blocking=True)
+        b_e.copy_(b_h, non_blocking=True)
+        lut_e.copy_(lut_h, non_blocking=True)
+        eng.pbs(a_e, b_e, lut_e, 1, oa_e, ob_e)
+        oa_h.copy_(oa_e, non_blocking=True)
+        ob_h.copy_(ob_e, non_blocking=True)
+
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_same = bool(torch.equal(oa_h, oa.cpu()) and torch.equal(ob_h, ob.cpu()))
+
+    # max over ranks
+    times = torch.tensor([dev_ms, e2e_ms, float(errors), 0.0 if e2e_same else 1.0], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    dev_ms, e2e_ms, errors_max, e2e_diff = times.tolist()
+    eng.close()
+    if rank != 0:
+        return None
+
+    total = B * args.steps * world
+    value = total / (dev_ms * 1e-3)
+    e2e_value = total / (e2e_ms * 1e-3)
+    fl = flops_per_pbs(p)
+    achieved_tf = B * fl / (br_ms * 1e-3) / 1e12
+    traffic = read_traffic(B)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(p, B), "params": p.name, "batch_per_gpu": B, "n_lut": 1,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "inputs larger than L2: 402 MB of ciphertexts and LUTs per step, 195 MB key"},
+        "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(a_h.numel() * 4 + b_h.numel() * 4 + lut_h.numel() * 4),
+                "d2h_bytes_per_step": int(oa_h.numel() * 4 + ob_h.numel() * 4),
+                "outputs_equal_device_arm": not bool(e2e_diff)},
+        "roofline": {"bound": "fp64", "achieved": round(achieved_tf, 3), "peak": round(peak_fp64, 3),
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / peak_fp64, 4), "traffic": traffic,
+                     "kernel": "br_fp64_kernel<11,2> (blind rotation + extraction)",
+                     "flops_per_pbs": int(fl), "launch_ms": round(br_ms, 3),
+                     "peak_source": "FP64 FMA probe (tfhe_probe_fp64_fma) on this GPU; MEASURED_PEAKS.json "
+                                    "holds no FP64 figure",
+                     "key_bytes_per_launch": p.bsk_bytes_fp64(),
+                     "key_stream_gbs": round(p.bsk_bytes_fp64() / (br_ms * 1e-3) / 1e9, 1)},
+        "kernels_ms": {"keyswitch": round(ks_ms, 3), "blind_rotate_extract": round(br_ms, 3)},
+        "decrypt_errors": int(errors_max), "decrypt_checked": B * world,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+    }
+    return line
+
+
+def read_traffic(batch):
+    """DRAM bytes per launch of the blind-rotation kernel from the committed
+    ncu summary (bytes per ciphertext of a captured launch), or None."""
+    path = os.path.join(ROOT, "profiles", "br_fp64_cfg2_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_ciphertext"):
+            return int(float(line.split("=")[1]) * batch)
+    return None
+
+
+# ---------------------------------------------------------------- CPU statement
+def _oracle_worker_init(seed):
+    global _W
+    import numpy as np
+    from oracle import tfhe_oracle as O
+    from tfhe_b200 import client
+    from tfhe_b200.params import CONFIG2
+    p = CONFIG2
+    keys = client.keygen(p, seed)
+    cen = lambda u: np.asarray(u, dtype=np.uint32).view(np.int32).astype(np.float64)
+    _W = dict(p=p, keys=keys, cen=cen, bo=O.bsk_coeff_fourier_ordered(cen(keys.bsk)),
+              rot=O.all_rot_possible_fourier(p.N), ksk=(cen(keys.ksk_a), cen(keys.ksk_b)[..., None]))
+
+
+def _oracle_pbs(chunk):
+    """KS + FP64 blind rotation + extraction of the numpy statement of the
+    reference (schemas/LWE_jax.py:97-117, schemas/RLWE_jax.py:288-303)."""
+    import numpy as np
+    from oracle import tfhe_oracle as O
+    from tfhe_b200 import client
+    w = _W
+    p, cen = w["p"], w["cen"]
+    a, b, lut = chunk
+    t0 = time.perf_counter()
+    ca, cb = O.key_switch_LWE(w["ksk"], (cen(a), cen(b)[:, None]),
+                              {"beta_ks": 2 ** p.log2_beta_ks, "l_ks": p.l_ks, "q": p.q})
+    oa, ob = O.cuboot_merge((ca, cb), [cen(lut[:, 0]), cen(lut[:, 1])], w["bo"], p.q, 2 ** p.log2_beta_bs,
+                            p.l_bs, p.N, p.collapse, w["rot"], 1)
+    dt = time.perf_counter() - t0
+    dec = client.decrypt(client._u32(oa[:, 0]), client._u32(ob[:, 0, 0]), w["keys"].sk_glwe, T_MSG)
+    return dt, dec
+
+
+class CpuStatement:
+    """Process pool (spawned before any GPU work) timing the numpy statement
+    of the path; every worker derives the same keys from the seed."""
+
+    def __init__(self, seed, workers):
+        import multiprocessing as mp
+        self.workers = workers
+        self.pool = mp.get_context("spawn").Pool(workers, initializer=_oracle_worker_init, initargs=(seed,))
+
+    def run(self, a, b, lut):
+        import numpy as np
+        w = self.workers
+        chunks = [(a[i::w], b[i::w], lut[i::w]) for i in range(w) if len(a[i::w])]
+        t0 = time.perf_counter()
+        res = self.pool.map(_oracle_pbs, chunks)
+        wall = time.perf_counter() - t0
+        dec = np.empty(len(a), dtype=np.int64)
+        for i, (_, d) in enumerate(res):
+            dec[i::w] = d
+        return wall, dec
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_sample(seed, count, workers):
+    """PBS/s of the numpy statement on `count` ciphertexts of the workload."""
+    import numpy as np
+    from tfhe_b200.params import CONFIG2
+    keys, msgs, a, b, lut, expect = make_inputs(CONFIG2, count, seed)
+    st = CpuStatement(seed, workers)
+    try:
+        st.run(a[:workers], b[:workers], lut[:workers])          # warm-up
+        wall, dec = st.run(a, b, lut)
+    finally:
+        st.close()
+    return count / wall, wall, int(np.sum(dec != expect))
+
+
+def _set_single_thread():
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the CPU statement of the path timed on the host
+    cores with all threads (one process per core), on the engine arm's
+    workload; each step is a bounded sample of one ciphertext per core."""
+    if rank != 0:
+        return None
+    import numpy as np
+    from tfhe_b200.params import CONFIG2
+    cores = os.cpu_count() or 1
+    steps = args.warmup + args.steps
+    keys, msgs, a, b, lut, expect = make_inputs(CONFIG2, cores * steps, args.seed)
+    st = CpuStatement(args.seed, cores)
+    walls, errors = [], 0
+    try:
+        for s in range(steps):
+            sl = slice(s * cores, (s + 1) * cores)
+            wall, dec = st.run(a[sl], b[sl], lut[sl])
+            if s >= args.warmup:
+                walls.append(wall)
+                errors += int(np.sum(dec != expect[sl]))
+    finally:
+        st.close()
+    wall = sum(walls)
+    value = cores * args.steps / wall
+    sample = f"{cores} ciphertexts per step (one per process) of the batch-{args.batch} workload"
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(CONFIG2, args.batch), "n_lut": 1},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample + "; numpy statement of the reference JAX path (oracle/)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "decrypt_errors": errors,
+        "note": "the reference's own CUDA kernel needs cuFFTDx and the XLA FFI headers, absent here; "
+                "its JAX path needs jax, absent here; the CPU arm is the numpy statement of that path",
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        _set_single_thread()
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # bounded CPU sample before any CUDA work (spawned workers)
+        _set_single_thread()
+        rate, wall, err = cpu_sample(args.seed + 99, args.cpu_sample, 1)
+        cpu = {"value": round(rate, 3), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_sample} ciphertexts of the same workload (key switch + FP64 blind rotation "
+                         f"+ extraction), numpy statement of the reference JAX path, 1 thread, {wall:.1f} s",
+               "decrypt_errors": err}
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    line = run_engine(args, rank, world, local_rank, dist)
+    if line is not None:
+        line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

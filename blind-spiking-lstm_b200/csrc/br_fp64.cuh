@@ -22,6 +22,10 @@
 
 namespace tfhe {
 
+// ciphertexts sharing one thread's key loads in the pointwise stage; the
+// CTA's ciphertext count K is always a multiple of it (launcher)
+constexpr int br_kt(int logn, int L) { return (L <= 2 && logn <= 11) ? 2 : 1; }
+
 struct BrArgs {
     const double2* bsk;       // native [G][2][P][M][H]; reference layout (G,2,L,2,M,H)
     const double2* all_rot;   // reference layout only: (2N, H)
@@ -46,6 +50,10 @@ struct BrArgs {
     uint32_t* out_a;          // (B, n_lut, N): extracted masks
     uint32_t* out_b;          // (B, n_lut)
     int64_t* out_i64;         // (B, 2, N): reference-layout result
+    // key ring (KR > 0): stages of the shared-memory ring, wait bound
+    int ring_stages;
+    long long wait_limit;     // clock cycles per mbarrier wait
+    int* status;              // device status word (tfhe_device_status)
 };
 
 // coefficient of X^e (any integer e) of a negacyclic polynomial in smem
@@ -87,13 +95,19 @@ __device__ __forceinline__ void forward_middle(double2* dec, int npoly, const do
     }
 }
 
-template <int LOGN, int L, bool REFLAYOUT>
-__global__ void __launch_bounds__(512, 1) br_fp64_kernel(const BrArgs args) {
+// KR = 0: key words read from global memory by every thread (any K).
+// KR > 0: K == KR ciphertexts per CTA and the key streamed through a
+// shared-memory ring by 1D bulk copies; the device key layout is then
+// [G][4/KR parts][2 out][M][P][NT slots] so each (group, part, out, pattern)
+// chunk of P * NT words is contiguous (NT = KR H / 4 = threads per CTA).
+template <int LOGN, int L, bool REFLAYOUT, int KR>
+__global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp64_kernel(const BrArgs args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
     constexpr int LOGH = LOGN - 1;
     constexpr int P = 2 * L;
     constexpr int Q8 = H / 8;
+    constexpr int KT = br_kt(LOGN, L);     // ciphertexts per thread in the pointwise stage
     using PL = Plan<LOGH>;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -105,6 +119,10 @@ __global__ void __launch_bounds__(512, 1) br_fp64_kernel(const BrArgs args) {
     uint16_t* freq = reinterpret_cast<uint16_t*>(tw + PL::TW);      // H
     int* rot = reinterpret_cast<int*>(freq + H);                    // K * M
     int* bexp = rot + K * M;                                        // K
+    // key ring: 128-byte aligned stages, then one mbarrier per stage
+    const size_t ring_off = ((reinterpret_cast<uintptr_t>(bexp + K) - reinterpret_cast<uintptr_t>(smem_raw)) + 127) & ~size_t(127);
+    double2* ring = reinterpret_cast<double2*>(smem_raw + ring_off);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ring + (size_t)(KR > 0 ? args.ring_stages : 0) * P * (KR * H / 4));
 
     const int tid = threadIdx.x;
     const int nt = blockDim.x;
@@ -113,6 +131,26 @@ __global__ void __launch_bounds__(512, 1) br_fp64_kernel(const BrArgs args) {
     for (int i = tid; i < N / 2; i += nt) qt[i] = args.qt[i];
     for (int i = tid; i < PL::TW; i += nt) tw[i] = args.tw[i];
     for (int i = tid; i < H; i += nt) freq[i] = args.freq[i];
+
+    // key ring: chunk q of the launch = key words [q * P * NT, (q+1) * P * NT)
+    constexpr int RNT = KR * H / 4;                 // threads (= slots per part) in ring mode
+    constexpr int NPART = KR > 0 ? 4 / KR : 1;
+    const int ring_nc = NPART * 2 * M;              // chunks per group
+    const long long ring_total = (long long)args.G * ring_nc;
+    const uint32_t ring_bytes = (uint32_t)(P * RNT * sizeof(double2));
+    if constexpr (KR > 0) {
+        if (tid == 0) {
+            for (int st = 0; st < args.ring_stages; ++st) mbar_init(&bars[st], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int st = 0; st < args.ring_stages && st < ring_total; ++st) {
+                mbar_arrive_expect_tx(&bars[st], ring_bytes);
+                bulk_load(ring + (size_t)st * P * RNT, args.bsk + (size_t)st * P * RNT, ring_bytes, &bars[st]);
+            }
+        }
+    }
 
     // the butterfly this thread owns in the first / last superstage
     const int ok = tid / (2 * Q8);
@@ -199,47 +237,129 @@ __global__ void __launch_bounds__(512, 1) br_fp64_kernel(const BrArgs args) {
         __syncthreads();
         forward_middle<LOGH, 1>(dec, K * P, tw, tid, nt);
 
-        // pointwise: out[a] = sum_m X^{r_m} * sum_bc BSK[g,a,bc,m] * DEC[bc]
-        {
-            const size_t gbase = (size_t)g * 2 * P * M * H;
-            for (int t = tid; t < K * H; t += nt) {
-                const int k = t % K;
-                const int p = t / K;
-                double2* pk = dec + (size_t)k * P * H;
-                double2 d[P];
+        if constexpr (KR > 0) {
+            // pointwise with the key streamed through the ring: chunk
+            // (part, out a, pattern m) holds the P key words of every slot of
+            // the part; thread tid owns slot part * NT + tid for all KR
+            // ciphertexts, so every staged key word is read once.
+            double2 d[KR][P];
+            double2 o0[KR], o1[KR];
+            int e = 0;
+            for (int c = 0; c < ring_nc; ++c) {
+                const long long qi = (long long)g * ring_nc + c;
+                const int st = (int)(qi % args.ring_stages);
+                const uint32_t par = (uint32_t)((qi / args.ring_stages) & 1);
+                const int part = c / (2 * M);
+                const int a = (c / M) & 1;
+                const int m = c % M;
+                const int p = part * RNT + tid;
+                if (a == 0 && m == 0) {
 #pragma unroll
-                for (int bc = 0; bc < P; ++bc) d[bc] = pk[bc * H + swz(p)];
-                const int j = freq[p];
-                const int e = 4 * j + 1;                       // evaluation point zeta^e
-                // reference layout index of the same point (or its conjugate)
-                const bool cj = REFLAYOUT && (e >= N);
-                const int jr = REFLAYOUT ? (cj ? (N - 1 - 2 * j) : 2 * j) : p;
-                double2 o0 = make_double2(0.0, 0.0), o1 = make_double2(0.0, 0.0);
-                const int* rk = rot + k * M;
-                for (int m = 0; m < M; ++m) {
-                    double2 w;
-                    if constexpr (REFLAYOUT) {
-                        w = __ldg(args.all_rot + (size_t)rk[m] * H + jr);
-                        if (cj) w = c_conj(w);
-                    } else {
-                        w = root2n<LOGN>(qt, rk[m] * e);
-                    }
-                    double2 t0 = make_double2(0.0, 0.0), t1 = make_double2(0.0, 0.0);
-                    const double2* b0 = args.bsk + gbase + (size_t)m * H + jr;
-                    const double2* b1 = b0 + (size_t)P * M * H;
+                    for (int kt = 0; kt < KR; ++kt) {
 #pragma unroll
-                    for (int bc = 0; bc < P; ++bc) {
-                        double2 k0 = __ldg(b0 + (size_t)bc * M * H);
-                        double2 k1 = __ldg(b1 + (size_t)bc * M * H);
-                        if (cj) { k0 = c_conj(k0); k1 = c_conj(k1); }
-                        c_mac(t0, k0, d[bc]);
-                        c_mac(t1, k1, d[bc]);
+                        for (int bc = 0; bc < P; ++bc) d[kt][bc] = dec[(size_t)kt * P * H + bc * H + swz(p)];
+                        o0[kt] = o1[kt] = make_double2(0.0, 0.0);
                     }
-                    c_mac(o0, w, t0);
-                    c_mac(o1, w, t1);
+                    e = 4 * freq[p] + 1;
                 }
-                pk[swz(p)] = o0;
-                pk[H + swz(p)] = o1;
+                mbar_wait_bounded(&bars[st], par, args.wait_limit, args.status);
+                const double2* chunk = ring + (size_t)st * P * RNT;
+                double2 t[KR];
+#pragma unroll
+                for (int kt = 0; kt < KR; ++kt) t[kt] = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int bc = 0; bc < P; ++bc) {
+                    const double2 kv = chunk[bc * RNT + tid];
+#pragma unroll
+                    for (int kt = 0; kt < KR; ++kt) c_mac(t[kt], kv, d[kt][bc]);
+                }
+#pragma unroll
+                for (int kt = 0; kt < KR; ++kt) {
+                    const double2 w = root2n<LOGN>(qt, rot[kt * M + m] * e);
+                    if (a == 0) c_mac(o0[kt], w, t[kt]);
+                    else c_mac(o1[kt], w, t[kt]);
+                }
+                if (a == 1 && m == M - 1) {
+#pragma unroll
+                    for (int kt = 0; kt < KR; ++kt) {
+                        dec[(size_t)kt * P * H + swz(p)] = o0[kt];
+                        dec[(size_t)kt * P * H + H + swz(p)] = o1[kt];
+                    }
+                }
+                __syncthreads();                      // stage st fully read
+                if (tid == 0 && qi + args.ring_stages < ring_total) {
+                    const long long qn = qi + args.ring_stages;
+                    fence_proxy_async_smem();
+                    mbar_arrive_expect_tx(&bars[st], ring_bytes);
+                    bulk_load(ring + (size_t)st * P * RNT, args.bsk + (size_t)qn * P * RNT, ring_bytes, &bars[st]);
+                }
+            }
+        } else {
+            // pointwise: out[a] = sum_m X^{r_m} * sum_bc BSK[g,a,bc,m] * DEC[bc].
+            // One thread per (slot, group of KT ciphertexts): every key word is
+            // loaded once into registers and used for KT ciphertexts.
+            {
+                const size_t gbase = (size_t)g * 2 * P * M * H;
+                const int KG = K / KT;
+                for (int t = tid; t < KG * H; t += nt) {
+                    const int kg = t % KG;
+                    const int p = t / KG;
+                    double2 d[KT][P];
+    #pragma unroll
+                    for (int kt = 0; kt < KT; ++kt)
+    #pragma unroll
+                        for (int bc = 0; bc < P; ++bc) d[kt][bc] = dec[(size_t)(kg * KT + kt) * P * H + bc * H + swz(p)];
+                    const int j = freq[p];
+                    const int e = 4 * j + 1;                       // evaluation point zeta^e
+                    // reference layout index of the same point (or its conjugate)
+                    const bool cj = REFLAYOUT && (e >= N);
+                    const int jr = REFLAYOUT ? (cj ? (N - 1 - 2 * j) : 2 * j) : p;
+                    double2 o0[KT], o1[KT];
+    #pragma unroll
+                    for (int kt = 0; kt < KT; ++kt) o0[kt] = o1[kt] = make_double2(0.0, 0.0);
+                    const double2* kb = args.bsk + gbase + jr;
+    #pragma unroll 1
+                    for (int m = 0; m < M; ++m) {
+                        double2 t0[KT], t1[KT];
+    #pragma unroll
+                        for (int kt = 0; kt < KT; ++kt) t0[kt] = t1[kt] = make_double2(0.0, 0.0);
+                        // all 2P key words of this pattern in flight before use
+                        double2 k0[P], k1[P];
+    #pragma unroll
+                        for (int bc = 0; bc < P; ++bc) {
+                            k0[bc] = __ldg(kb + ((size_t)bc * M + m) * H);
+                            k1[bc] = __ldg(kb + ((size_t)(P + bc) * M + m) * H);
+                        }
+    #pragma unroll
+                        for (int bc = 0; bc < P; ++bc) {
+                            if (cj) { k0[bc] = c_conj(k0[bc]); k1[bc] = c_conj(k1[bc]); }
+    #pragma unroll
+                            for (int kt = 0; kt < KT; ++kt) {
+                                c_mac(t0[kt], k0[bc], d[kt][bc]);
+                                c_mac(t1[kt], k1[bc], d[kt][bc]);
+                            }
+                        }
+    #pragma unroll
+                        for (int kt = 0; kt < KT; ++kt) {
+                            const int r = rot[(kg * KT + kt) * M + m];
+                            double2 w;
+                            if constexpr (REFLAYOUT) {
+                                w = __ldg(args.all_rot + (size_t)r * H + jr);
+                                if (cj) w = c_conj(w);
+                            } else {
+                                w = root2n<LOGN>(qt, r * e);
+                            }
+                            c_mac(o0[kt], w, t0[kt]);
+                            c_mac(o1[kt], w, t1[kt]);
+                        }
+                    }
+    #pragma unroll
+                    for (int kt = 0; kt < KT; ++kt) {
+                        double2* pk = dec + (size_t)(kg * KT + kt) * P * H;
+                        pk[swz(p)] = o0[kt];
+                        pk[H + swz(p)] = o1[kt];
+                    }
+                }
             }
         }
         __syncthreads();
@@ -336,6 +456,7 @@ struct BskConvArgs {
     const double2* tw;
     int G, M, L;
     long long npoly;   // 2 * 2 * G * M * L
+    int ring_nt;       // 0: [G][2][P][M][H]; > 0: [G][H/ring_nt][2][M][P][ring_nt]
 };
 
 template <int LOGN>
@@ -373,7 +494,15 @@ __global__ void __launch_bounds__(256) bsk_fft_kernel(const BskConvArgs a) {
         const long long g = gm / a.M;
         const int m = (int)(gm % a.M);
         const int bc = lvl * 2 + in;
-        a.dst[(((g * 2 + out) * P + bc) * a.M + m) * H + p] = buf[lp * H + swz(p)];
+        size_t di;
+        if (a.ring_nt > 0) {
+            const int parts = H / a.ring_nt;
+            di = ((((size_t)g * parts + p / a.ring_nt) * 2 + out) * a.M + m) * P + bc;
+            di = di * a.ring_nt + p % a.ring_nt;
+        } else {
+            di = (((size_t)(g * 2 + out) * P + bc) * a.M + m) * H + p;
+        }
+        a.dst[di] = buf[lp * H + swz(p)];
     }
 }
 

@@ -12,14 +12,20 @@
 
 namespace tfhe {
 
-BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout) {
+BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr) {
+#define TFHE_BR_CASE(LL)                                                             \
+    case LL:                                                                         \
+        if (reflayout) return br_fp64_kernel<BR_LOGN, LL, true, 0>;                  \
+        if (kr == 2) return br_fp64_kernel<BR_LOGN, LL, false, 2>;                   \
+        return kr == 0 ? br_fp64_kernel<BR_LOGN, LL, false, 0> : nullptr;
     switch (L) {
-        case 1: return reflayout ? br_fp64_kernel<BR_LOGN, 1, true> : br_fp64_kernel<BR_LOGN, 1, false>;
-        case 2: return reflayout ? br_fp64_kernel<BR_LOGN, 2, true> : br_fp64_kernel<BR_LOGN, 2, false>;
-        case 3: return reflayout ? br_fp64_kernel<BR_LOGN, 3, true> : br_fp64_kernel<BR_LOGN, 3, false>;
-        case 4: return reflayout ? br_fp64_kernel<BR_LOGN, 4, true> : br_fp64_kernel<BR_LOGN, 4, false>;
+        TFHE_BR_CASE(1)
+        TFHE_BR_CASE(2)
+        TFHE_BR_CASE(3)
+        TFHE_BR_CASE(4)
         default: return nullptr;
     }
+#undef TFHE_BR_CASE
 }
 
 BrConvKernel TFHE_CAT(bsk_fft_logn_, BR_LOGN)() { return bsk_fft_kernel<BR_LOGN>; }

@@ -24,6 +24,7 @@ struct tfhe_keys {
     int ldk = 0;
     const tfhe::FftPlan* plan = nullptr;
     int64_t bytes = 0;
+    int ring_kr = 0;            // > 0: key in the ring layout for K == ring_kr per CTA
 };
 
 namespace tfhe {
@@ -122,6 +123,23 @@ static void build_tables(int N, std::vector<double2>& qt, std::vector<double2>& 
 
 static std::mutex g_plan_mu;
 static std::map<std::pair<int, int>, FftPlan*> g_plans;   // (device, N)
+static std::map<int, int*> g_status;                      // device -> status word
+
+// the device status word kernels write on a bounded-wait timeout
+static int* device_status_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_status.find(dev);
+    if (it != g_status.end()) return it->second;
+    int* w = nullptr;
+    if (cudaMalloc(&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess) {
+        cudaFree(w);
+        return nullptr;
+    }
+    g_status[dev] = w;
+    return w;
+}
 
 const FftPlan* get_plan(int N) {
     int dev = 0;
@@ -177,16 +195,22 @@ static int max_smem_optin() {
 struct BrShape {
     int K = 0, nt = 0;
     size_t smem = 0;
+    int kr = 0, stages = 0;   // key ring (kr > 0)
 };
+
+// a mbarrier wait gives up after this many cycles (about 2 s)
+constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL;
 
 static BrShape br_shape(int N, int L, int M, long long B) {
     const int H = N / 2, Q8 = H / 8;
+    const int KT = br_kt(ilog2(N), L);
     const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
     const size_t limit = (size_t)max_smem_optin();
     BrShape s;
     int K = std::max(1, 512 / (2 * Q8));
     K = (int)std::min<long long>(K, std::max<long long>(B, 1));
-    while (K >= 1) {
+    K = std::max(KT, K / KT * KT);
+    while (K >= KT) {
         const size_t smem = per_ct * K + br_table_bytes(N) + (size_t)(K * M + K) * sizeof(int) + 16;
         if (smem <= limit) {
             s.K = K;
@@ -194,16 +218,44 @@ static BrShape br_shape(int N, int L, int M, long long B) {
             s.smem = smem;
             return s;
         }
-        --K;
+        K -= KT;
     }
     return s;
 }
 
-static int launch_br(BrArgs args, int N, int L, bool reflayout, cudaStream_t stream) {
+// Key-ring shape: K = KR = 2 ciphertexts per CTA, NT = KR H / 4 threads,
+// chunks of 2L * NT key words, as many stages (2..4) as shared memory holds.
+// Opt-in with TFHE_B200_KEY_RING=1 when the keys are created: on B200 the
+// per-thread loads of the plain kernel are merged across SMs at L2 (all CTAs
+// walk the key in lockstep) while bulk copies are not, so the plain kernel
+// is faster for the workloads measured here.
+static BrShape ring_shape(int N, int L, int M) {
+    BrShape s;
+    const char* env = getenv("TFHE_B200_KEY_RING");
+    if (!env || env[0] != '1') return s;
+    const int H = N / 2, KR = 2, P = 2 * L;
+    const int nt = KR * H / 4;
+    if (nt < 64 || nt > 512 || KR * P > 12) return s;
+    const size_t chunk = (size_t)P * nt * sizeof(double2);
+    size_t base = (size_t)KR * P * H * sizeof(double2) + br_table_bytes(N) + (size_t)(KR * M + KR) * sizeof(int);
+    base = (base + 127) & ~(size_t)127;
+    const size_t limit = (size_t)max_smem_optin();
+    if (base + 2 * (chunk + 8) > limit) return s;
+    const int stages = (int)std::min<size_t>(4, (limit - base) / (chunk + 8));
+    s.K = KR;
+    s.nt = nt;
+    s.kr = KR;
+    s.stages = stages;
+    s.smem = base + stages * chunk + stages * 8;
+    return s;
+}
+
+static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream) {
     const int logn = ilog2(N);
-    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout);
+    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
-    const BrShape sh = br_shape(N, L, args.M, args.B);
+    const BrShape sh = kr > 0 ? ring_shape(N, L, args.M) : br_shape(N, L, args.M, args.B);
+    if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
     if (sh.K < 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT,
                     "degree " + std::to_string(N) + " with l=" + std::to_string(L) +
@@ -214,6 +266,10 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, cudaStream_t str
     args.tw = pl->tw;
     args.freq = pl->freq;
     args.K = sh.K;
+    args.ring_stages = sh.stages;
+    args.wait_limit = WAIT_LIMIT_CYCLES;
+    args.status = device_status_word();
+    if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word allocation failed");
     TFHE_TRY(check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sh.smem),
                         "cudaFuncSetAttribute(blind rotation)"));
@@ -384,6 +440,35 @@ __global__ void rotate_extract_i64_kernel(const int64_t* __restrict__ acc, const
     }
 }
 
+// FP64 FMA throughput probe: 8 independent chains per thread
+__global__ void fp64_fma_probe_kernel(int iters, double* out) {
+    double a[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = 1.0 + 1e-9 * (threadIdx.x + i);
+    const double m = 0.999999999, c = 1e-12;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i] = fma(a[i], m, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += a[i];
+    if (s == 12345.678) out[0] = s;   // keeps the chains live
+}
+
+// waits on a barrier that nothing arrives on: the bounded wait must give
+// up after `limit` cycles and record the timeout in *status
+__global__ void wait_timeout_probe_kernel(long long limit, int* status, int* result) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, limit, status);
+    if (threadIdx.x == 0) *result = ok ? 1 : 0;
+}
+
 // ---------------------------------------------------------------- validation
 static int validate_params(const tfhe_params* p) {
     if (!p) return fail(TFHE_ERR_INVALID_ARGUMENT, "params is NULL");
@@ -447,6 +532,7 @@ static int keys_common(const tfhe_params* params, tfhe_keys** out, tfhe_keys** m
         delete k;
         return TFHE_ERR_INTERNAL;
     }
+    k->ring_kr = ring_shape(params->N, params->l_bs, k->M).kr;
     *made = k;
     return TFHE_OK;
 }
@@ -508,7 +594,7 @@ int tfhe_mul_bootstrap(void* stream, const int64_t* ct_init, int64_t ct_elems, c
     a.indices = indices;
     a.out_i64 = out;
     a.n_lut = 1;
-    return launch_br(a, (int)degree, (int)l, true, static_cast<cudaStream_t>(stream));
+    return launch_br(a, (int)degree, (int)l, true, 0, static_cast<cudaStream_t>(stream));
 }
 
 int tfhe_keys_create(const tfhe_params* params, const uint32_t* bsk_coeff, const uint32_t* ksk_a,
@@ -533,7 +619,8 @@ int tfhe_keys_create(const tfhe_params* params, const uint32_t* bsk_coeff, const
         rc = check_cuda(cudaMemcpyAsync(d_src, bsk_coeff, src_bytes, cudaMemcpyHostToDevice, stream), "bsk upload");
     }
     if (rc == TFHE_OK) {
-        BskConvArgs ca{d_src, k->bsk, k->plan->qt, k->plan->tw, k->G, k->M, L, npoly};
+        BskConvArgs ca{d_src, k->bsk, k->plan->qt, k->plan->tw, k->G, k->M, L, npoly,
+                       k->ring_kr > 0 ? k->ring_kr * H / 4 : 0};
         const int ppc = std::max(1, 2048 / H);
         const size_t smem = (size_t)ppc * H * sizeof(double2);
         BrConvKernel kern = bsk_fft_kernel_for(ilog2(N));
@@ -580,11 +667,19 @@ int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordere
                 for (int c = 0; c < 2; ++c)
                     for (int m = 0; m < M; ++m) {
                         const double2* row = src + ((((size_t)a * 2 + c) * L + lvl) * ((size_t)G * M) + (size_t)g * M + m) * H;
-                        double2* dst = host.data() + ((((size_t)g * 2 + a) * P + lvl * 2 + c) * M + m) * H;
+                        const int rnt = k->ring_kr > 0 ? k->ring_kr * H / 4 : 0;
+                        const int bc = lvl * 2 + c;
                         for (int pp = 0; pp < H; ++pp) {
                             const int j = freq[pp];
                             const int e = 4 * j + 1;
-                            dst[pp] = e < N ? row[2 * j] : make_double2(row[N - 1 - 2 * j].x, -row[N - 1 - 2 * j].y);
+                            size_t di;
+                            if (rnt > 0) {
+                                di = ((((size_t)g * (H / rnt) + pp / rnt) * 2 + a) * M + m) * P + bc;
+                                di = di * rnt + pp % rnt;
+                            } else {
+                                di = ((((size_t)g * 2 + a) * P + bc) * M + m) * H + pp;
+                            }
+                            host[di] = e < N ? row[2 * j] : make_double2(row[N - 1 - 2 * j].x, -row[N - 1 - 2 * j].y);
                         }
                     }
     int rc = check_cuda(cudaMalloc(&k->bsk, total * sizeof(double2)), "cudaMalloc(bsk)");
@@ -638,7 +733,7 @@ static int br_native(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_
     a.acc_out = acc_out;
     a.out_a = out_a;
     a.out_b = out_b;
-    return launch_br(a, p.N, p.l_bs, false, stream);
+    return launch_br(a, p.N, p.l_bs, false, keys->ring_kr, stream);
 }
 
 int tfhe_blind_rotate(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
@@ -664,6 +759,17 @@ int tfhe_sample_extract(const uint32_t* acc, int32_t N, int32_t n_lut, uint32_t*
     return check_cuda(cudaGetLastError(), "sample extract launch");
 }
 
+int tfhe_cuboot_merge(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
+                      int64_t lut_count, int32_t n_lut, uint32_t* out_a, uint32_t* out_b, int64_t batch,
+                      void* stream) {
+    TFHE_TRY(check_keys(keys));
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!lwe_a || !lwe_b || !lut || !out_a || !out_b) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    return br_native(keys, lwe_a, lwe_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch,
+                     static_cast<cudaStream_t>(stream));
+}
+
 int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, const uint32_t* lut,
              int64_t lut_count, int32_t n_lut, uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream_v) {
     TFHE_TRY(check_keys(keys));
@@ -681,6 +787,42 @@ int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, 
         rc = br_native(keys, ks, ks_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch, stream);
     const int rc2 = check_cuda(cudaFreeAsync(ks, stream), "cudaFreeAsync(key-switch output)");
     return rc != TFHE_OK ? rc : rc2;
+}
+
+int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* scratch, double* flops,
+                        void* stream) {
+    if (blocks < 1 || threads < 1 || threads > 1024 || iters < 1 || !scratch || !flops)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "invalid probe shape");
+    *flops = 2.0 * 8.0 * (double)blocks * threads * iters;
+    fp64_fma_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(iters, scratch);
+    return check_cuda(cudaGetLastError(), "fp64 probe launch");
+}
+
+int tfhe_device_status(int32_t* status_out, int32_t clear) {
+    if (!status_out) return fail(TFHE_ERR_INVALID_ARGUMENT, "status_out is NULL");
+    int* w = device_status_word();
+    if (!w) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
+    int v = 0;
+    TFHE_TRY(check_cuda(cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost), "read device status"));
+    *status_out = v;
+    if (clear) TFHE_TRY(check_cuda(cudaMemset(w, 0, sizeof(int)), "clear device status"));
+    return TFHE_OK;
+}
+
+int tfhe_probe_wait_timeout(int64_t limit_cycles, int32_t* waited_out) {
+    if (limit_cycles < 1 || limit_cycles > 4000000000LL || !waited_out)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "limit must be in [1, 4e9] cycles");
+    int* w = device_status_word();
+    if (!w) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
+    int* res = nullptr;
+    TFHE_TRY(check_cuda(cudaMalloc(&res, sizeof(int)), "cudaMalloc(probe)"));
+    wait_timeout_probe_kernel<<<1, 32>>>(limit_cycles, w, res);
+    int rc = check_cuda(cudaGetLastError(), "timeout probe launch");
+    int v = -1;
+    if (rc == TFHE_OK) rc = check_cuda(cudaMemcpy(&v, res, sizeof(int), cudaMemcpyDeviceToHost), "timeout probe");
+    cudaFree(res);
+    *waited_out = v;
+    return rc;
 }
 
 int tfhe_keyswitch_ref(const uint32_t* a_in, const uint32_t* b_in, const uint32_t* ksk_a, const uint32_t* ksk_b,

@@ -85,12 +85,11 @@ __device__ __forceinline__ double2 root2n(const double2* qt, int idx) {
     idx &= (2 * N - 1);
     const int quad = idx >> (LOGN - 1);
     const double2 w = qt[idx & (N / 2 - 1)];
-    switch (quad) {
-        case 0: return w;
-        case 1: return make_double2(w.y, -w.x);
-        case 2: return make_double2(-w.x, -w.y);
-        default: return make_double2(-w.y, w.x);
-    }
+    // multiply by (-i)^quad with selects (lanes take different quadrants)
+    const bool odd = quad & 1, neg = quad & 2;
+    const double x = odd ? w.y : w.x;
+    const double y = odd ? -w.x : w.y;
+    return neg ? make_double2(-x, -y) : make_double2(x, y);
 }
 
 // ----------------------------------------------------------------------------
@@ -221,6 +220,72 @@ __device__ __forceinline__ void stage_all(double2* polys, int npoly, const doubl
         if (INV) dit_stage<R, S>(poly, tw, t % PER);
         else dif_stage<R, S>(poly, tw, t % PER);
     }
+}
+
+// ----------------------------------------------------------------------------
+// asynchronous bulk copies (TMA, 1D, no multicast) and mbarriers
+// ----------------------------------------------------------------------------
+// device status word values (tfhe_device_status)
+constexpr int TFHE_STATUS_WAIT_TIMEOUT = 1;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// make barrier initialisation visible to the async (TMA) proxy
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// order this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy writes to the same buffer
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared bulk copy completing `bytes` of transaction on `bar`;
+// dst, src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// wait for phase `parity` of `bar` for at most `limit` clock cycles; on
+// timeout record TFHE_STATUS_WAIT_TIMEOUT in *status and return false (the
+// caller carries on, so every thread still reaches every barrier)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit, int* status) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > limit) {
+            if (status) atomicExch(status, TFHE_STATUS_WAIT_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
 }
 
 // ----------------------------------------------------------------------------

@@ -150,6 +150,22 @@ class Keys:
                                                  n_lut, _ptr(acc_out), B, _stream(stream)))
         return acc_out
 
+    def cuboot_merge(self, lwe_a, lwe_b, lut, n_lut=1, out_a=None, out_b=None, stream=None):
+        """cuboot_merge from key-switched LWEs: lwe (B, n) / (B), lut
+        (1|B, 2, N) -> out_a (B, n_lut, N), out_b (B, n_lut)."""
+        p = self.params
+        B = lwe_a.shape[0]
+        _need(lwe_a, torch.int32, (B, p.n), "lwe_a")
+        _need(lwe_b, torch.int32, (B,), "lwe_b")
+        _need(lut, torch.int32, (lut.shape[0], 2, p.N), "lut")
+        out_a = out_a if out_a is not None else torch.empty((B, n_lut, p.N), dtype=torch.int32, device=lwe_a.device)
+        out_b = out_b if out_b is not None else torch.empty((B, n_lut), dtype=torch.int32, device=lwe_a.device)
+        _need(out_a, torch.int32, (B, n_lut, p.N), "out_a")
+        _need(out_b, torch.int32, (B, n_lut), "out_b")
+        _lib.check(_lib.load().tfhe_cuboot_merge(self.handle, _ptr(lwe_a), _ptr(lwe_b), _ptr(lut), lut.shape[0],
+                                                 n_lut, _ptr(out_a), _ptr(out_b), B, _stream(stream)))
+        return out_a, out_b
+
     def pbs(self, a, b, lut, n_lut=1, out_a=None, out_b=None, stream=None):
         """Key switch + blind rotation + many-LUT extraction
         (HeavysideBoostrapper.cuboot): a (B, n_big), b (B), lut (1|B, 2, N)
@@ -177,3 +193,25 @@ def sample_extract(acc, n_lut=1, out_a=None, out_b=None, stream=None):
     _lib.check(_lib.load().tfhe_sample_extract(_ptr(acc), N, n_lut, _ptr(out_a), _ptr(out_b), B,
                                                _stream(stream)))
     return out_a, out_b
+
+
+def probe_fp64_peak(iters=4096, reps=5) -> float:
+    """Measured FP64 FMA throughput of the current device in TFLOP/s (best
+    of ``reps`` launches of 8 independent FMA chains per thread, 8 CTAs of
+    512 threads per SM)."""
+    dev = torch.cuda.current_device()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    scratch = torch.zeros(1, dtype=torch.float64, device="cuda")
+    flops = ctypes.c_double()
+    lib = _lib.load()
+    s = _stream()
+    best = 0.0
+    for i in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(lib.tfhe_probe_fp64_fma(sms * 8, 512, iters, _ptr(scratch), ctypes.byref(flops), s))
+        e1.record()
+        torch.cuda.synchronize()
+        if i:
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best

@@ -123,6 +123,14 @@ int tfhe_blind_rotate(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32
 int tfhe_sample_extract(const uint32_t* acc, int32_t N, int32_t n_lut,
                         uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
 
+/* The steps of cuboot_merge (schemas/RLWE_jax.py:288-303) from
+ * key-switched LWEs: blind rotation from the LUT, rotation by -b~, many-LUT
+ * extraction.  lwe_a (batch, n), lwe_b (batch), lut (lut_count, 2, N)
+ * -> out_a (batch, n_lut, N), out_b (batch, n_lut). */
+int tfhe_cuboot_merge(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b,
+                      const uint32_t* lut, int64_t lut_count, int32_t n_lut,
+                      uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
+
 /* Full programmable bootstrap: key switch, blind rotation, rotation by -b~
  * and many-LUT extraction, HeavysideBoostrapper.cuboot
  * (nn_tfhe/activation.py:148-162) = cuboot_merge(key_switch_LWE(h)).
@@ -152,6 +160,26 @@ int tfhe_keyswitch_ref(const uint32_t* a_in, const uint32_t* b_in,
 int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int32_t n_lut,
                             int64_t log2_q, int64_t* out_acc, int64_t* out_a, int64_t* out_b,
                             int64_t batch, void* stream);
+
+/* Status word of the current device: kernels that wait on an mbarrier
+ * give up after a bounded time and record TFHE_DEVICE_TIMEOUT here instead
+ * of hanging (no counterpart in the reference).  clear != 0 resets it. */
+#define TFHE_DEVICE_TIMEOUT 1
+int tfhe_device_status(int32_t* status_out, int32_t clear);
+
+/* Diagnostics (no counterpart in the reference): runs one bounded mbarrier
+ * wait that nothing completes, with a limit of limit_cycles clock cycles;
+ * *waited_out = 0 when it gave up (the device status then reads
+ * TFHE_DEVICE_TIMEOUT).  Synchronous. */
+int tfhe_probe_wait_timeout(int64_t limit_cycles, int32_t* waited_out);
+
+/* Diagnostics (no counterpart in the reference): FP64 FMA throughput
+ * probe for the roofline denominator.  Launches blocks x threads threads,
+ * each running 8 independent FMA chains of `iters` steps; *flops receives
+ * the flop count of the launch (host pointer); scratch is one device
+ * double.  Time it with events on `stream`. */
+int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* scratch,
+                        double* flops, void* stream);
 
 #ifdef __cplusplus
 }

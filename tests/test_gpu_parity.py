@@ -206,6 +206,31 @@ def test_mul_bootstrap_dropin_matches_reference_path(name, batch):
     assert np.array_equal(got1.cpu().numpy(), want)
 
 
+@pytest.mark.parametrize("name", ["tiny_c3", "cfg1", "cfg2"])
+def test_key_ring_and_plain_paths_agree(name, monkeypatch):
+    """The key-ring kernel (keys in the chunked layout, bulk copies) and the
+    plain kernel give identical outputs."""
+    p = PARAMS[name]
+    k = keys(name)
+    t = 32 if p["beta_bs"] <= 2 ** 7 else 16
+    msgs, a, b = inputs(name, 5, t=t)
+    lut = device_u32(np.stack([np.zeros(p["N"]), step_body(name, t=t)])[None])
+    outs = []
+    for ring in ("1", "0"):
+        monkeypatch.setenv("TFHE_B200_KEY_RING", ring)   # read when the keys are created
+        e = Keys.create(pset(name), k.bsk_coeff, k.ksk[0], k.ksk[1].reshape(k.ksk[1].shape[:2]))
+        outs.append(e.pbs(device_u32(a), device_u32(b.reshape(-1)), lut))
+        e.close()
+    if p["beta_bs"] <= 2 ** 7:
+        assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    else:
+        # beta = 2^15: FFT rounding may differ in the last unit; decryptions agree
+        for oa, ob in outs:
+            dec = O.decrypt_LWE((centred(host_u32(oa)[:, 0]), centred(host_u32(ob)[:, 0])), k.sk_glwe,
+                                {"t": t, "q": p["q"]})
+            assert np.array_equal(dec, (msgs >= t // 4).astype(float))
+
+
 def test_fourier_key_upload_equals_coefficient_upload():
     name = "tiny_c3"
     k = keys(name)
@@ -298,3 +323,30 @@ def test_reference_golden_fixtures(name, batch, n_lut):
     assert np.array_equal(u32(kk[0].cpu().numpy()), u32(G[f"{name}_ks_a"]))
     assert np.array_equal(u32(kk[1].cpu().numpy()), u32(G[f"{name}_ks_b"]))
     eng.close()
+
+
+def test_bounded_wait_gives_up_and_reports():
+    """A wait that nothing completes returns after its limit and sets the
+    device status word; the context stays usable."""
+    import ctypes
+    from tfhe_b200 import _lib
+    lib = _lib.load()
+    st = ctypes.c_int32()
+    _lib.check(lib.tfhe_device_status(ctypes.byref(st), 1))
+    waited = ctypes.c_int32(-1)
+    _lib.check(lib.tfhe_probe_wait_timeout(2_000_000, ctypes.byref(waited)))
+    assert waited.value == 0
+    _lib.check(lib.tfhe_device_status(ctypes.byref(st), 1))
+    assert st.value == 1
+    _lib.check(lib.tfhe_device_status(ctypes.byref(st), 0))
+    assert st.value == 0
+    # the device still runs the engine afterwards
+    test_standalone_extract_and_rotate_ops()
+
+
+def test_no_wait_timeouts_recorded():
+    import ctypes
+    from tfhe_b200 import _lib
+    st = ctypes.c_int32()
+    _lib.check(_lib.load().tfhe_device_status(ctypes.byref(st), 0))
+    assert st.value == 0
