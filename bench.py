@@ -33,6 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "blind-spiking-lstm_b200"))
 METRIC = "PBS/s (key switch + blind rotation + many-LUT extraction) at 0 decrypt errors"
 UNIT = "PBS/s"
 T_MSG = 16           # Z_8 messages with a padding bit: phase m q / 16
+T_OUT = 8            # table outputs in Z_8 at scale q / 8 (final outputs, no padding bit)
 N_TABLES = 8
 
 
@@ -73,7 +74,7 @@ def make_inputs(p, batch, seed):
     a, b = client.encrypt(keys, msgs, T_MSG, rng)
     tables = rng.integers(0, T_MSG // 2, size=(N_TABLES, T_MSG // 2))
     which = rng.integers(0, N_TABLES, size=batch)
-    bodies = np.stack([client.table_lut(p.N, tables[i], T_MSG) for i in range(N_TABLES)])
+    bodies = np.stack([client.table_lut(p.N, tables[i], T_OUT) for i in range(N_TABLES)])
     lut = np.zeros((batch, 2, p.N), dtype=np.uint32)
     lut[:, 1] = bodies[which]
     expect = tables[which, msgs]
@@ -192,8 +193,11 @@ def run_engine(args, rank, world, local_rank, dist):
     # decryption check of the device outputs
     out_a = oa.cpu().numpy().view(np.uint32)[:, 0]
     out_b = ob.cpu().numpy().view(np.uint32)[:, 0]
-    dec = client.decrypt(out_a, out_b, keys.sk_glwe, T_MSG)
+    dec = client.decrypt(out_a, out_b, keys.sk_glwe, T_OUT)
     errors = int(np.sum(dec != expect))
+    noise = client.phase(out_a, out_b, keys.sk_glwe) - expect.astype(np.int64) * (2 ** 32 // T_OUT)
+    noise = ((noise + 2 ** 31) % 2 ** 32) - 2 ** 31
+    noise_log2_std = float(np.log2(np.std(noise.astype(np.float64))))
 
     # end to end through tfhe_pbs with host buffers
     oa_h = torch.empty((B, 1, p.N), dtype=torch.int32).pin_memory()
@@ -262,6 +266,7 @@ def run_engine(args, rank, world, local_rank, dist):
                      "key_stream_gbs": round(p.bsk_bytes_fp64() / (br_ms * 1e-3) / 1e9, 1)},
         "kernels_ms": {"keyswitch": round(ks_ms, 3), "blind_rotate_extract": round(br_ms, 3)},
         "decrypt_errors": int(errors_max), "decrypt_checked": B * world,
+        "output_noise_log2_std": round(noise_log2_std, 2),
         "gpu_launches": 2 * args.steps,
         "clocks": clk,
     }
@@ -309,7 +314,7 @@ def _oracle_pbs(chunk):
     oa, ob = O.cuboot_merge((ca, cb), [cen(lut[:, 0]), cen(lut[:, 1])], w["bo"], p.q, 2 ** p.log2_beta_bs,
                             p.l_bs, p.N, p.collapse, w["rot"], 1)
     dt = time.perf_counter() - t0
-    dec = client.decrypt(client._u32(oa[:, 0]), client._u32(ob[:, 0, 0]), w["keys"].sk_glwe, T_MSG)
+    dec = client.decrypt(client._u32(oa[:, 0]), client._u32(ob[:, 0, 0]), w["keys"].sk_glwe, T_OUT)
     return dt, dec
 
 
