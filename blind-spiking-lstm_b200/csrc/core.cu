@@ -250,7 +250,8 @@ static BrShape ring_shape(int N, int L, int M) {
     return s;
 }
 
-static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream) {
+static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream,
+                     int* status = nullptr) {
     const int logn = ilog2(N);
     BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
@@ -268,7 +269,7 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     args.K = sh.K;
     args.ring_stages = sh.stages;
     args.wait_limit = WAIT_LIMIT_CYCLES;
-    args.status = device_status_word();
+    args.status = status ? status : device_status_word();
     if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word allocation failed");
     TFHE_TRY(check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sh.smem),
@@ -712,7 +713,7 @@ int tfhe_keyswitch(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* 
 
 static int br_native(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
                      int64_t lut_count, int32_t n_lut, uint32_t* acc_out, uint32_t* out_a, uint32_t* out_b,
-                     int64_t batch, cudaStream_t stream) {
+                     int64_t batch, cudaStream_t stream, int* status = nullptr) {
     const tfhe_params& p = keys->p;
     if (n_lut < 1 || n_lut > p.N) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut must be in [1, N]");
     if (lut_count != 1 && lut_count != batch) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut_count must be 1 or batch");
@@ -733,7 +734,7 @@ static int br_native(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_
     a.acc_out = acc_out;
     a.out_a = out_a;
     a.out_b = out_b;
-    return launch_br(a, p.N, p.l_bs, false, keys->ring_kr, stream);
+    return launch_br(a, p.N, p.l_bs, false, keys->ring_kr, stream, status);
 }
 
 int tfhe_blind_rotate(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
@@ -853,6 +854,65 @@ int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int3
     rotate_extract_i64_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         acc, b, N, n_lut, std::ldexp(1.0, (int)log2_q), out_acc, out_a, out_b, batch);
     return check_cuda(cudaGetLastError(), "rotate/extract launch");
+}
+
+// ---------------------------------------------------------------------------
+// Programmable bootstrap without any allocation.  The key-switched LWEs that
+// tfhe_pbs keeps in a stream-ordered allocation live here in a fixed static
+// device array instead, for callers that must not allocate device memory:
+// an XLA custom call whose runtime has preallocated most of the GPU, a
+// serving loop that forbids allocation on its latency path, or code running
+// under an external memory manager.  Every GPU that loads the library holds
+// this array until the process exits.  Word 0 of the header is the status
+// word of the call (bounded-wait timeouts of the key-ring kernel).
+// ---------------------------------------------------------------------------
+constexpr size_t NOALLOC_HEADER_WORDS = 64;                       // 256 bytes
+constexpr size_t NOALLOC_SCRATCH_WORDS = (size_t(8) << 20) / 4;   // 8 MiB of key-switched LWEs
+static __device__ __align__(256) uint32_t g_pbs_noalloc_scratch[NOALLOC_HEADER_WORDS + NOALLOC_SCRATCH_WORDS];
+
+static std::mutex g_noalloc_mu;
+static std::map<int, uint32_t*> g_noalloc_base;   // device -> address of the array
+
+// device address of the static array for the current device (looked up
+// once per device; the host-side symbol itself is not a device address)
+static int noalloc_base(uint32_t** out) {
+    int dev = 0;
+    TFHE_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    auto it = g_noalloc_base.find(dev);
+    if (it == g_noalloc_base.end()) {
+        uint32_t* ptr = nullptr;
+        TFHE_TRY(check_cuda(cudaGetSymbolAddress((void**)&ptr, g_pbs_noalloc_scratch),
+                            "cudaGetSymbolAddress(no-allocation scratch)"));
+        it = g_noalloc_base.emplace(dev, ptr).first;
+    }
+    *out = it->second;
+    return TFHE_OK;
+}
+
+int tfhe_pbs_noalloc(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, const uint32_t* lut,
+                     int64_t lut_count, int32_t n_lut, uint32_t* out_a, uint32_t* out_b, int64_t batch,
+                     void* stream_v) {
+    TFHE_TRY(check_keys(keys));
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!a_in || !b_in || !lut || !out_a || !out_b) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    const size_t n = (size_t)keys->p.n;
+    const size_t max_batch = NOALLOC_SCRATCH_WORDS / (n + 1);
+    if ((size_t)batch > max_batch)
+        return fail(TFHE_ERR_INVALID_ARGUMENT,
+                    "tfhe_pbs_noalloc: batch " + std::to_string(batch) + " exceeds the static scratch of " +
+                        std::to_string(NOALLOC_SCRATCH_WORDS * 4) + " bytes (at most " + std::to_string(max_batch) +
+                        " ciphertexts for n = " + std::to_string(n) + "); split the batch or use tfhe_pbs");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    uint32_t* base = nullptr;
+    TFHE_TRY(noalloc_base(&base));
+    int* status = reinterpret_cast<int*>(base);
+    uint32_t* ks = base + NOALLOC_HEADER_WORDS;
+    uint32_t* ks_b = ks + (size_t)batch * n;
+    TFHE_TRY(check_cuda(cudaMemsetAsync(status, 0, sizeof(int), stream), "clear status word"));
+    TFHE_TRY(launch_ks(keys, a_in, b_in, ks, ks_b, batch, stream));
+    return br_native(keys, ks, ks_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch, stream, status);
 }
 
 }  // extern "C"

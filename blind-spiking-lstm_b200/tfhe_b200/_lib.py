@@ -45,6 +45,7 @@ SIGNATURES = {
     "tfhe_blind_rotate": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _I64, _P]),
     "tfhe_sample_extract": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I64, _P]),
     "tfhe_pbs": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _P]),
+    "tfhe_pbs_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _P]),
     "tfhe_cuboot_merge": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _P]),
     "tfhe_probe_fp64_fma": (ctypes.c_int, [_I32, _I32, _I32, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "tfhe_device_status": (ctypes.c_int, [ctypes.POINTER(_I32), _I32]),

@@ -141,6 +141,22 @@ int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in,
              const uint32_t* lut, int64_t lut_count, int32_t n_lut,
              uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
 
+/* tfhe_pbs without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: an XLA custom call
+ * (XLA preallocates most of the GPU for its own allocator), a serving loop
+ * that forbids allocation on its latency path, code under an external
+ * memory manager.  The key-switched intermediate lives in a static 8 MiB
+ * device array of the library, so batch * (n + 1) * 4 bytes must fit in it
+ * (at most 2822 ciphertexts for n = 742, 3323 for n = 630); larger batches
+ * return TFHE_ERR_INVALID_ARGUMENT.  The array's device address is looked up
+ * on the first call on each device (call once before any stream capture).
+ * Every call shares the one array: calls that overlap on the GPU (other
+ * streams, other threads) race and corrupt each other's results.  Same
+ * arguments and results as tfhe_pbs. */
+int tfhe_pbs_noalloc(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in,
+                     const uint32_t* lut, int64_t lut_count, int32_t n_lut,
+                     uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
+
 /* key_switch_LWE (schemas/LWE_jax.py:97-117) with the key in the
  * reference's own layout, as DEVICE uint32 arrays: ksk_a (l_ks, n_big, n)
  * and ksk_b (l_ks, n_big) (the pk / b of get_keyswitch_sk_LWE modulo 2^32).
