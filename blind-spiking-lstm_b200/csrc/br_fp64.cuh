@@ -24,7 +24,7 @@ namespace tfhe {
 
 // ciphertexts sharing one thread's key loads in the pointwise stage; the
 // CTA's ciphertext count K is always a multiple of it (launcher)
-constexpr int br_kt(int logn, int L) { return (L <= 2 && logn <= 11) ? 2 : 1; }
+constexpr int br_kt(int logn, int L) { return (L <= 3 && logn <= 11) ? 2 : 1; }
 
 struct BrArgs {
     const double2* bsk;       // native [G][2][P][M][H]; reference layout (G,2,L,2,M,H)
@@ -52,6 +52,7 @@ struct BrArgs {
     int64_t* out_i64;         // (B, 2, N): reference-layout result
     // key ring (KR > 0): stages of the shared-memory ring, wait bound
     int ring_stages;
+    int prefetch;             // L1 prefetch of the next pattern's key words: 1 on, 0 off, -1 by path
     long long wait_limit;     // clock cycles per mbarrier wait
     int* status;              // device status word (tfhe_device_status)
 };
@@ -100,14 +101,14 @@ __device__ __forceinline__ void forward_middle(double2* dec, int npoly, const do
 // shared-memory ring by 1D bulk copies; the device key layout is then
 // [G][4/KR parts][2 out][M][P][NT slots] so each (group, part, out, pattern)
 // chunk of P * NT words is contiguous (NT = KR H / 4 = threads per CTA).
-template <int LOGN, int L, bool REFLAYOUT, int KR>
+template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP>
 __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp64_kernel(const BrArgs args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
     constexpr int LOGH = LOGN - 1;
     constexpr int P = 2 * L;
     constexpr int Q8 = H / 8;
-    constexpr int KT = br_kt(LOGN, L);     // ciphertexts per thread in the pointwise stage
+    constexpr int KT = KTP;                // ciphertexts per thread in the pointwise stage
     using PL = Plan<LOGH>;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -126,7 +127,10 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 
     const int tid = threadIdx.x;
     const int nt = blockDim.x;
-    const long long ct0 = (long long)blockIdx.x * K;
+    // persistent CTAs: this CTA takes ciphertext sets blockIdx.x, +gridDim.x, ...
+    // so every SM walks the key in lockstep for the whole launch
+    const long long nsets = (args.B + K - 1) / K;
+    const long long my_sets = blockIdx.x < nsets ? (nsets - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
     for (int i = tid; i < N / 2; i += nt) qt[i] = args.qt[i];
     for (int i = tid; i < PL::TW; i += nt) tw[i] = args.tw[i];
@@ -136,7 +140,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     constexpr int RNT = KR * H / 4;                 // threads (= slots per part) in ring mode
     constexpr int NPART = KR > 0 ? 4 / KR : 1;
     const int ring_nc = NPART * 2 * M;              // chunks per group
-    const long long ring_total = (long long)args.G * ring_nc;
+    const long long ring_set = (long long)args.G * ring_nc;   // chunks per ciphertext set
+    const long long ring_total = my_sets * ring_set;          // chunks this CTA consumes
     const uint32_t ring_bytes = (uint32_t)(P * RNT * sizeof(double2));
     if constexpr (KR > 0) {
         if (tid == 0) {
@@ -147,7 +152,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
         if (tid == 0) {
             for (int st = 0; st < args.ring_stages && st < ring_total; ++st) {
                 mbar_arrive_expect_tx(&bars[st], ring_bytes);
-                bulk_load(ring + (size_t)st * P * RNT, args.bsk + (size_t)st * P * RNT, ring_bytes, &bars[st]);
+                bulk_load(ring + (size_t)st * P * RNT, args.bsk + (size_t)(st % ring_set) * P * RNT, ring_bytes,
+                          &bars[st]);
             }
         }
     }
@@ -156,12 +162,15 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     const int ok = tid / (2 * Q8);
     const int oa = (tid / Q8) & 1;
     const int on1 = tid % Q8;
-    const long long oct = min(ct0 + ok, args.B - 1);
 
     const double q = ldexp(1.0, args.log2_q);
     const double inv_q = ldexp(1.0, -args.log2_q);
     const double beta = ldexp(1.0, args.log2_beta);
     constexpr double inv_h = 1.0 / H;
+
+    for (long long iter = 0; iter < my_sets; ++iter) {
+    const long long ct0 = (blockIdx.x + iter * gridDim.x) * K;
+    const long long oct = min(ct0 + ok, args.B - 1);
 
     double acc_lo[8], acc_hi[8];
     if constexpr (REFLAYOUT) {
@@ -213,6 +222,10 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                 x_hi[n2] = acc_hi[n2] * inv_q;
             }
             double2* pk = dec + (size_t)ok * P * H + oa * H;
+            double2 w0[8];
+            w0[0] = make_double2(1.0, 0.0);
+#pragma unroll
+            for (int k2 = 1; k2 < 8; ++k2) w0[k2] = tw[(k2 - 1) * Q8 + on1];
 #pragma unroll
             for (int lvl = 0; lvl < L; ++lvl) {
                 double2 v[8];
@@ -228,7 +241,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                     v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
                 }
                 dft8<false>(v);
-                twiddle<8, Q8, false>(v, tw, on1);
+#pragma unroll
+                for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
                 double2* poly = pk + lvl * 2 * H;
 #pragma unroll
                 for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[k2];
@@ -246,7 +260,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             double2 o0[KR], o1[KR];
             int e = 0;
             for (int c = 0; c < ring_nc; ++c) {
-                const long long qi = (long long)g * ring_nc + c;
+                const long long qi = iter * ring_set + (long long)g * ring_nc + c;
                 const int st = (int)(qi % args.ring_stages);
                 const uint32_t par = (uint32_t)((qi / args.ring_stages) & 1);
                 const int part = c / (2 * M);
@@ -291,7 +305,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                     const long long qn = qi + args.ring_stages;
                     fence_proxy_async_smem();
                     mbar_arrive_expect_tx(&bars[st], ring_bytes);
-                    bulk_load(ring + (size_t)st * P * RNT, args.bsk + (size_t)qn * P * RNT, ring_bytes, &bars[st]);
+                    bulk_load(ring + (size_t)st * P * RNT, args.bsk + (size_t)(qn % ring_set) * P * RNT, ring_bytes,
+                              &bars[st]);
                 }
             }
         } else {
@@ -318,39 +333,81 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     #pragma unroll
                     for (int kt = 0; kt < KT; ++kt) o0[kt] = o1[kt] = make_double2(0.0, 0.0);
                     const double2* kb = args.bsk + gbase + jr;
-    #pragma unroll 1
+#pragma unroll 1
                     for (int m = 0; m < M; ++m) {
-                        double2 t0[KT], t1[KT];
-    #pragma unroll
-                        for (int kt = 0; kt < KT; ++kt) t0[kt] = t1[kt] = make_double2(0.0, 0.0);
-                        // all 2P key words of this pattern in flight before use
-                        double2 k0[P], k1[P];
-    #pragma unroll
-                        for (int bc = 0; bc < P; ++bc) {
-                            k0[bc] = __ldg(kb + ((size_t)bc * M + m) * H);
-                            k1[bc] = __ldg(kb + ((size_t)(P + bc) * M + m) * H);
-                        }
-    #pragma unroll
-                        for (int bc = 0; bc < P; ++bc) {
-                            if (cj) { k0[bc] = c_conj(k0[bc]); k1[bc] = c_conj(k1[bc]); }
-    #pragma unroll
-                            for (int kt = 0; kt < KT; ++kt) {
-                                c_mac(t0[kt], k0[bc], d[kt][bc]);
-                                c_mac(t1[kt], k1[bc], d[kt][bc]);
+                        if (args.prefetch > 0 || (args.prefetch < 0 && 2 * P * KT > 16)) {
+                            // next pattern of this slot, or the first pattern of
+                            // this thread's next slot: into L1 while this one computes
+                            const double2* nb = kb + (size_t)(m + 1) * H;
+                            if (m + 1 == M) {
+                                const int tn = t + nt;
+                                const int pn = tn / KG;
+                                nb = (tn < KG * H) ? args.bsk + gbase + (REFLAYOUT ? 0 : pn) : nullptr;
+                                if (REFLAYOUT) nb = nullptr;
+                            }
+                            if (nb) {
+#pragma unroll
+                                for (int bc = 0; bc < 2 * P; ++bc) prefetch_l1(nb + (size_t)bc * M * H);
                             }
                         }
-    #pragma unroll
+                        double2 w[KT];
+#pragma unroll
                         for (int kt = 0; kt < KT; ++kt) {
                             const int r = rot[(kg * KT + kt) * M + m];
-                            double2 w;
                             if constexpr (REFLAYOUT) {
-                                w = __ldg(args.all_rot + (size_t)r * H + jr);
-                                if (cj) w = c_conj(w);
+                                w[kt] = __ldg(args.all_rot + (size_t)r * H + jr);
+                                if (cj) w[kt] = c_conj(w[kt]);
                             } else {
-                                w = root2n<LOGN>(qt, r * e);
+                                w[kt] = root2n<LOGN>(qt, r * e);
                             }
-                            c_mac(o0[kt], w, t0[kt]);
-                            c_mac(o1[kt], w, t1[kt]);
+                        }
+                        if constexpr (2 * P * KT <= 16) {
+                            // both outputs' key words of this pattern in flight before use
+                            double2 k0[P], k1[P];
+#pragma unroll
+                            for (int bc = 0; bc < P; ++bc) {
+                                k0[bc] = __ldg(kb + ((size_t)bc * M + m) * H);
+                                k1[bc] = __ldg(kb + ((size_t)(P + bc) * M + m) * H);
+                            }
+                            double2 t0[KT], t1[KT];
+#pragma unroll
+                            for (int kt = 0; kt < KT; ++kt) t0[kt] = t1[kt] = make_double2(0.0, 0.0);
+#pragma unroll
+                            for (int bc = 0; bc < P; ++bc) {
+                                if (cj) { k0[bc] = c_conj(k0[bc]); k1[bc] = c_conj(k1[bc]); }
+#pragma unroll
+                                for (int kt = 0; kt < KT; ++kt) {
+                                    c_mac(t0[kt], k0[bc], d[kt][bc]);
+                                    c_mac(t1[kt], k1[bc], d[kt][bc]);
+                                }
+                            }
+#pragma unroll
+                            for (int kt = 0; kt < KT; ++kt) {
+                                c_mac(o0[kt], w[kt], t0[kt]);
+                                c_mac(o1[kt], w[kt], t1[kt]);
+                            }
+                        } else {
+                            // one output at a time: P key words in flight
+#pragma unroll
+                            for (int a = 0; a < 2; ++a) {
+                                double2 kv[P];
+#pragma unroll
+                                for (int bc = 0; bc < P; ++bc) kv[bc] = __ldg(kb + ((size_t)(a * P + bc) * M + m) * H);
+                                double2 t[KT];
+#pragma unroll
+                                for (int kt = 0; kt < KT; ++kt) t[kt] = make_double2(0.0, 0.0);
+#pragma unroll
+                                for (int bc = 0; bc < P; ++bc) {
+                                    if (cj) kv[bc] = c_conj(kv[bc]);
+#pragma unroll
+                                    for (int kt = 0; kt < KT; ++kt) c_mac(t[kt], kv[bc], d[kt][bc]);
+                                }
+#pragma unroll
+                                for (int kt = 0; kt < KT; ++kt) {
+                                    if (a == 0) c_mac(o0[kt], w[kt], t[kt]);
+                                    else c_mac(o1[kt], w[kt], t[kt]);
+                                }
+                            }
                         }
                     }
     #pragma unroll
@@ -438,6 +495,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                 args.out_b[(ct0 + k) * nl + al] = ncoef<LOGN>(acc + (size_t)k * 2 * N + N, al + bexp[k]);
             }
         }
+    }
+    __syncthreads();               // shared memory is reused by the next set
     }
 }
 

@@ -12,12 +12,14 @@
 
 namespace tfhe {
 
-BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr) {
-#define TFHE_BR_CASE(LL)                                                             \
-    case LL:                                                                         \
-        if (reflayout) return br_fp64_kernel<BR_LOGN, LL, true, 0>;                  \
-        if (kr == 2) return br_fp64_kernel<BR_LOGN, LL, false, 2>;                   \
-        return kr == 0 ? br_fp64_kernel<BR_LOGN, LL, false, 0> : nullptr;
+BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt) {
+#define TFHE_BR_CASE(LL)                                                                         \
+    case LL:                                                                                     \
+        if (reflayout) return kt == 2 ? br_fp64_kernel<BR_LOGN, LL, true, 0, 2>                    \
+                                      : br_fp64_kernel<BR_LOGN, LL, true, 0, 1>;                   \
+        if (kr == 2) return br_fp64_kernel<BR_LOGN, LL, false, 2, 1>;                             \
+        if (kr != 0) return nullptr;                                                             \
+        return kt == 2 ? br_fp64_kernel<BR_LOGN, LL, false, 0, 2> : br_fp64_kernel<BR_LOGN, LL, false, 0, 1>;
     switch (L) {
         TFHE_BR_CASE(1)
         TFHE_BR_CASE(2)

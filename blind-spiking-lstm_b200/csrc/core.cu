@@ -64,9 +64,8 @@ static bool is_pow2(long long v) { return v > 0 && (v & (v - 1)) == 0; }
 
 // radix sequence of an H = 2^logh point transform (same as Plan<LOGH>)
 static std::vector<int> radices(int logh) {
-    std::vector<int> r(logh / 3, 8);
-    if (logh % 3 == 1) r.push_back(2);
-    if (logh % 3 == 2) r.push_back(4);
+    std::vector<int> r;
+    for (int st = 0; st < plan_stages(logh); ++st) r.push_back(plan_radix(logh, st));
     return r;
 }
 
@@ -177,6 +176,19 @@ size_t br_table_bytes(int N) {
            (size_t)H * sizeof(uint16_t);
 }
 
+static int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
 static int max_smem_optin() {
     static int cached[64] = {0};
     int dev = 0;
@@ -196,26 +208,38 @@ struct BrShape {
     int K = 0, nt = 0;
     size_t smem = 0;
     int kr = 0, stages = 0;   // key ring (kr > 0)
+    int kt = 1;               // ciphertexts per thread in the pointwise stage
 };
 
 // a mbarrier wait gives up after this many cycles (about 2 s)
 constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL;
 
+// ciphertexts per CTA: as many as 512 threads and shared memory allow, or
+// TFHE_B200_K (tuning: K = 1 lets two CTAs share an SM)
+static int k_override() {
+    static const int v = [] {
+        const char* env = getenv("TFHE_B200_K");
+        return env ? atoi(env) : 0;
+    }();
+    return v;
+}
+
 static BrShape br_shape(int N, int L, int M, long long B) {
     const int H = N / 2, Q8 = H / 8;
-    const int KT = br_kt(ilog2(N), L);
     const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
     const size_t limit = (size_t)max_smem_optin();
     BrShape s;
     int K = std::max(1, 512 / (2 * Q8));
+    if (k_override() > 0) K = std::min(K, k_override());
     K = (int)std::min<long long>(K, std::max<long long>(B, 1));
-    K = std::max(KT, K / KT * KT);
+    const int KT = (K % 2 == 0 && br_kt(ilog2(N), L) == 2) ? 2 : 1;
     while (K >= KT) {
         const size_t smem = per_ct * K + br_table_bytes(N) + (size_t)(K * M + K) * sizeof(int) + 16;
         if (smem <= limit) {
             s.K = K;
             s.nt = K * 2 * Q8;
             s.smem = smem;
+            s.kt = (K % KT == 0) ? KT : 1;
             return s;
         }
         K -= KT;
@@ -253,10 +277,10 @@ static BrShape ring_shape(int N, int L, int M) {
 static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream,
                      int* status = nullptr) {
     const int logn = ilog2(N);
-    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr);
-    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M) : br_shape(N, L, args.M, args.B);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
+    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt);
+    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
     if (sh.K < 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT,
                     "degree " + std::to_string(N) + " with l=" + std::to_string(L) +
@@ -269,12 +293,31 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     args.K = sh.K;
     args.ring_stages = sh.stages;
     args.wait_limit = WAIT_LIMIT_CYCLES;
+    // L1 prefetch of the next pattern's key words: by default where a thread
+    // loads one output's key words at a time (measured +5% there, -4% where
+    // both outputs' words are already in flight); TFHE_B200_PREFETCH=0/1 forces
+    static const int prefetch = [] {
+        const char* env = getenv("TFHE_B200_PREFETCH");
+        return env ? (env[0] == '1' ? 1 : 0) : -1;
+    }();
+    args.prefetch = prefetch;
     args.status = status ? status : device_status_word();
     if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word allocation failed");
     TFHE_TRY(check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sh.smem),
                         "cudaFuncSetAttribute(blind rotation)"));
-    const long long grid = (args.B + sh.K - 1) / sh.K;
+    // persistent CTAs: one per SM (shared memory admits one) looping over
+    // ciphertext sets, so all SMs walk the key in lockstep; environment
+    // TFHE_B200_PERSISTENT=0 launches one CTA per set instead (tuning)
+    const long long sets = (args.B + sh.K - 1) / sh.K;
+    static const bool persistent = [] {
+        const char* env = getenv("TFHE_B200_PERSISTENT");
+        return !(env && env[0] == '0');
+    }();
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sh.nt, sh.smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const long long grid = persistent ? std::min<long long>(sets, (long long)sm_count() * per_sm) : sets;
     kern<<<(unsigned)grid, sh.nt, sh.smem, stream>>>(args);
     return check_cuda(cudaGetLastError(), "blind rotation launch");
 }

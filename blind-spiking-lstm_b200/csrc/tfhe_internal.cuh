@@ -49,15 +49,27 @@ __device__ __forceinline__ double2 c_mul_mi(double2 a) { return make_double2(a.y
 __device__ __forceinline__ double2 c_mul_pi(double2 a) { return make_double2(-a.y, a.x); }
 
 // ----------------------------------------------------------------------------
-// radix plan: H = 2^h points as radix-8 superstages then one radix-2 or -4
+// radix plan of an H = 2^h point transform: the first superstage is radix 8
+// (the register-resident stage of the blind rotation), the others radix 8
+// or 16, as few superstages as possible:
+//   H = 64: 8.8   128: 8.16   256: 8.8.4   512: 8.8.8   1024: 8.8.16   2048: 8.16.16
 // ----------------------------------------------------------------------------
+constexpr int plan_stages(int logh) { return logh <= 7 ? 2 : 3; }
+constexpr int plan_radix(int logh, int s) {
+    return logh == 6 ? 8
+         : logh == 7 ? (s == 0 ? 8 : 16)
+         : logh == 8 ? (s < 2 ? 8 : 4)
+         : logh == 9 ? 8
+         : logh == 10 ? (s < 2 ? 8 : 16)
+         : (s == 0 ? 8 : 16);                       // logh == 11
+}
+
 template <int LOGH>
 struct Plan {
+    static_assert(LOGH >= 6 && LOGH <= 11, "transform size H = 64 .. 2048");
     static constexpr int H = 1 << LOGH;
-    static constexpr int N8 = LOGH / 3;             // radix-8 superstages
-    static constexpr int REM = LOGH % 3;            // 0, 1 (radix 2) or 2 (radix 4)
-    static constexpr int NS = N8 + (REM ? 1 : 0);   // superstages
-    static constexpr int radix(int s) { return s < N8 ? 8 : (REM == 1 ? 2 : 4); }
+    static constexpr int NS = plan_stages(LOGH);    // superstages
+    static constexpr int radix(int s) { return plan_radix(LOGH, s); }
     // span of superstage s (elements between the inputs of one butterfly)
     static constexpr int span(int s) {
         int prod = 1;
@@ -153,9 +165,46 @@ __device__ __forceinline__ void dft8(double2 (&v)[8]) {
     v[4] = c[1]; v[5] = c[5]; v[6] = c[3]; v[7] = c[7];
 }
 
+// exp(-+ i pi m / 8), m = 0..7
+__device__ __forceinline__ double2 w16(int m, bool inv) {
+    constexpr double C[8] = {1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173,
+                             0.0, -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613};
+    constexpr double S[8] = {0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613,
+                             1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173};
+    return make_double2(C[m], inv ? S[m] : -S[m]);
+}
+
+// 16-point DFT: four radix-2 DIF stages with constant twiddles, then the
+// bit-reversal permutation
+template <bool INV>
+__device__ __forceinline__ void dft16(double2 (&v)[16]) {
+#pragma unroll
+    for (int half = 8; half >= 1; half >>= 1) {
+#pragma unroll
+        for (int blk = 0; blk < 16; blk += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                const double2 a = v[blk + j], b = v[blk + j + half];
+                v[blk + j] = c_add(a, b);
+                const double2 d = c_sub(a, b);
+                const int m = j * (8 / half);                 // angle pi * m / 8
+                if (m == 0) v[blk + j + half] = d;
+                else if (m == 4) v[blk + j + half] = INV ? c_mul_pi(d) : c_mul_mi(d);
+                else v[blk + j + half] = c_mul(d, w16(m, INV));
+            }
+        }
+    }
+    double2 t[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) t[k] = v[((k & 1) << 3) | ((k & 2) << 1) | ((k & 4) >> 1) | ((k & 8) >> 3)];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = t[k];
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft(double2 (&v)[R]) {
-    if constexpr (R == 8) dft8<INV>(v);
+    if constexpr (R == 16) dft16<INV>(v);
+    else if constexpr (R == 8) dft8<INV>(v);
     else if constexpr (R == 4) dft4<INV>(v);
     else dft2<INV>(v[0], v[1]);
 }
@@ -207,6 +256,31 @@ __device__ __forceinline__ void dit_stage(double2* poly, const double2* tw, int 
 }
 
 // superstage s over `npoly` consecutive polynomials, spread over the CTA
+// one butterfly with its twiddles already in registers
+template <int R, int S, bool INV>
+__device__ __forceinline__ void stage_bfly(double2* poly, const double2 (&w)[R], int b) {
+    const int n1 = b % S;
+    const int base = (b / S) * R * S + n1;
+    double2 v[R];
+    if (!INV) {
+#pragma unroll
+        for (int n2 = 0; n2 < R; ++n2) v[n2] = poly[swz(base + S * n2)];
+        dft<R, false>(v);
+#pragma unroll
+        for (int k2 = 1; k2 < R; ++k2) v[k2] = c_mul(v[k2], w[k2]);
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) poly[swz(base + S * k2)] = v[k2];
+    } else {
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) v[k2] = poly[swz(base + S * k2)];
+#pragma unroll
+        for (int k2 = 1; k2 < R; ++k2) v[k2] = c_mul(v[k2], c_conj(w[k2]));
+        dft<R, true>(v);
+#pragma unroll
+        for (int n2 = 0; n2 < R; ++n2) poly[swz(base + S * n2)] = v[n2];
+    }
+}
+
 template <int LOGH, int s, bool INV>
 __device__ __forceinline__ void stage_all(double2* polys, int npoly, const double2* tw_all, int tid, int nt) {
     using P = Plan<LOGH>;
@@ -215,6 +289,17 @@ __device__ __forceinline__ void stage_all(double2* polys, int npoly, const doubl
     constexpr int PER = P::H / R;
     const double2* tw = tw_all + P::tw_offset(s);
     const int total = npoly * PER;
+    if (S > 1 && R <= 8 && nt % PER == 0) {
+        // every task of this thread is the same butterfly of another
+        // polynomial: load its twiddles once
+        const int b = tid % PER;
+        double2 w[R];
+        w[0] = make_double2(1.0, 0.0);
+#pragma unroll
+        for (int k2 = 1; k2 < R; ++k2) w[k2] = tw[(k2 - 1) * S + b % S];
+        for (int t = tid; t < total; t += nt) stage_bfly<R, S, INV>(polys + (t / PER) * P::H, w, b);
+        return;
+    }
     for (int t = tid; t < total; t += nt) {
         double2* poly = polys + (t / PER) * P::H;
         if (INV) dit_stage<R, S>(poly, tw, t % PER);
@@ -230,6 +315,10 @@ constexpr int TFHE_STATUS_WAIT_TIMEOUT = 1;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
