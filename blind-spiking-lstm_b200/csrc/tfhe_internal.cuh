@@ -85,9 +85,11 @@ struct Plan {
     static constexpr int TW = tw_offset(NS);        // total per-stage twiddles
 };
 
-// XOR swizzle of 16-byte elements inside 128-byte rows: strided butterfly
-// accesses of every superstage hit distinct bank groups.
-__device__ __forceinline__ int swz(int e) { return e ^ ((e >> 3) & 7); }
+// XOR swizzle of 16-byte elements inside 128-byte rows (row r = e >> 3,
+// column e & 7 XOR (r ^ r >> 1) & 7): the warp accesses of every superstage
+// (strides 1, 2, 4, 8 and 16 elements, spans 8..128) and of the pointwise
+// stage take the minimum of 4 wavefronts per 32 16-byte requests.
+__device__ __forceinline__ int swz(int e) { return e ^ (((e >> 3) ^ (e >> 4)) & 7); }
 
 // exp(-i pi idx / N) for any idx, from the quarter table qt[r] =
 // exp(-i pi r / N), r in [0, N/2)
