@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -25,6 +26,7 @@ struct tfhe_keys {
     const tfhe::FftPlan* plan = nullptr;
     int64_t bytes = 0;
     int ring_kr = 0;            // > 0: key in the ring layout for K == ring_kr per CTA
+    tfhe_tuning tune = {0, -1, -1};   // launch shape of the blind rotation (0 / -1: automatic)
 };
 
 namespace tfhe {
@@ -224,13 +226,14 @@ static int k_override() {
     return v;
 }
 
-static BrShape br_shape(int N, int L, int M, long long B) {
+static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0) {
     const int H = N / 2, Q8 = H / 8;
     const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
     const size_t limit = (size_t)max_smem_optin();
     BrShape s;
     int K = std::max(1, 512 / (2 * Q8));
-    if (k_override() > 0) K = std::min(K, k_override());
+    const int kreq = k_request > 0 ? k_request : k_override();
+    if (kreq > 0) K = std::min(K, kreq);
     K = (int)std::min<long long>(K, std::max<long long>(B, 1));
     const int KT = (K % 2 == 0 && br_kt(ilog2(N), L) == 2) ? 2 : 1;
     while (K >= KT) {
@@ -274,10 +277,38 @@ static BrShape ring_shape(int N, int L, int M) {
     return s;
 }
 
+// kernel attributes set once per kernel (also keeps launches capturable in a
+// CUDA graph after the first, uncaptured launch) and occupancy per shape
+static std::mutex g_attr_mu;
+static std::map<std::pair<int, const void*>, int> g_attr_smem;
+static std::map<std::tuple<int, const void*, int, size_t>, int> g_occupancy;
+
+static int prepare_kernel(const void* kern, int nt, size_t smem, int* per_sm) {
+    int dev = 0;
+    TFHE_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    int& have = g_attr_smem[{dev, kern}];
+    if (have < (int)smem) {
+        TFHE_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(blind rotation)"));
+        have = (int)smem;
+    }
+    auto key = std::make_tuple(dev, kern, nt, smem);
+    auto it = g_occupancy.find(key);
+    if (it == g_occupancy.end()) {
+        int v = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, nt, smem) != cudaSuccess || v < 1) v = 1;
+        it = g_occupancy.emplace(key, v).first;
+    }
+    *per_sm = it->second;
+    return TFHE_OK;
+}
+
 static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream,
-                     int* status = nullptr) {
+                     int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
-    const BrShape sh = kr > 0 ? ring_shape(N, L, args.M) : br_shape(N, L, args.M, args.B);
+    const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
+                              : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
     BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
@@ -296,27 +327,24 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     // L1 prefetch of the next pattern's key words: by default where a thread
     // loads one output's key words at a time (measured +5% there, -4% where
     // both outputs' words are already in flight); TFHE_B200_PREFETCH=0/1 forces
-    static const int prefetch = [] {
+    static const int prefetch_env = [] {
         const char* env = getenv("TFHE_B200_PREFETCH");
         return env ? (env[0] == '1' ? 1 : 0) : -1;
     }();
-    args.prefetch = prefetch;
+    args.prefetch = (tune && tune->prefetch >= 0) ? tune->prefetch : prefetch_env;
     args.status = status ? status : device_status_word();
     if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word allocation failed");
-    TFHE_TRY(check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sh.smem),
-                        "cudaFuncSetAttribute(blind rotation)"));
-    // persistent CTAs: one per SM (shared memory admits one) looping over
-    // ciphertext sets, so all SMs walk the key in lockstep; environment
-    // TFHE_B200_PERSISTENT=0 launches one CTA per set instead (tuning)
+    int per_sm = 1;
+    TFHE_TRY(prepare_kernel((const void*)kern, sh.nt, sh.smem, &per_sm));
+    // persistent CTAs: as many as fit on the SMs, looping over ciphertext
+    // sets, so all SMs walk the key in lockstep; TFHE_B200_PERSISTENT=0 (or
+    // the keys' tuning) launches one CTA per set instead
     const long long sets = (args.B + sh.K - 1) / sh.K;
-    static const bool persistent = [] {
+    static const bool persistent_env = [] {
         const char* env = getenv("TFHE_B200_PERSISTENT");
         return !(env && env[0] == '0');
     }();
-    int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sh.nt, sh.smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
+    const bool persistent = (tune && tune->persistent >= 0) ? tune->persistent != 0 : persistent_env;
     const long long grid = persistent ? std::min<long long>(sets, (long long)sm_count() * per_sm) : sets;
     kern<<<(unsigned)grid, sh.nt, sh.smem, stream>>>(args);
     return check_cuda(cudaGetLastError(), "blind rotation launch");
@@ -777,7 +805,7 @@ static int br_native(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_
     a.acc_out = acc_out;
     a.out_a = out_a;
     a.out_b = out_b;
-    return launch_br(a, p.N, p.l_bs, false, keys->ring_kr, stream, status);
+    return launch_br(a, p.N, p.l_bs, false, keys->ring_kr, stream, status, &keys->tune);
 }
 
 int tfhe_blind_rotate(const tfhe_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b, const uint32_t* lut,
@@ -840,6 +868,33 @@ int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* 
     *flops = 2.0 * 8.0 * (double)blocks * threads * iters;
     fp64_fma_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(iters, scratch);
     return check_cuda(cudaGetLastError(), "fp64 probe launch");
+}
+
+int tfhe_keys_set_tuning(tfhe_keys* keys, const tfhe_tuning* tuning) {
+    if (!keys) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys is NULL");
+    if (!tuning) {
+        keys->tune = tfhe_tuning{0, -1, -1};
+        return TFHE_OK;
+    }
+    if (tuning->ciphertexts_per_cta < 0 || tuning->ciphertexts_per_cta > 64 || tuning->prefetch < -1 ||
+        tuning->prefetch > 1 || tuning->persistent < -1 || tuning->persistent > 1)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "tuning out of range");
+    keys->tune = *tuning;
+    return TFHE_OK;
+}
+
+int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* ciphertexts_per_cta,
+                           int32_t* threads, int64_t* shared_bytes) {
+    if (!keys || !ciphertexts_per_cta || !threads || !shared_bytes)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL argument");
+    const tfhe_params& p = keys->p;
+    const BrShape sh = keys->ring_kr > 0 ? ring_shape(p.N, p.l_bs, keys->M)
+                                         : br_shape(p.N, p.l_bs, keys->M, std::max<int64_t>(batch, 1),
+                                                    keys->tune.ciphertexts_per_cta);
+    *ciphertexts_per_cta = sh.K;
+    *threads = sh.nt;
+    *shared_bytes = (int64_t)sh.smem;
+    return sh.K > 0 ? TFHE_OK : fail(TFHE_ERR_INVALID_ARGUMENT, "no launch shape fits");
 }
 
 int tfhe_device_status(int32_t* status_out, int32_t clear) {

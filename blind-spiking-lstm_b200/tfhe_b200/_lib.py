@@ -23,6 +23,11 @@ class TFHEError(RuntimeError):
         super().__init__(f"{self.status_name}: {message}")
 
 
+class TfheTuning(ctypes.Structure):
+    _fields_ = [("ciphertexts_per_cta", ctypes.c_int32), ("prefetch", ctypes.c_int32),
+                ("persistent", ctypes.c_int32)]
+
+
 class TfheParams(ctypes.Structure):
     _fields_ = [(name, ctypes.c_int32) for name in
                 ("N", "n", "n_big", "log2_beta_bs", "l_bs", "collapse", "log2_beta_ks", "l_ks", "log2_q")]
@@ -40,6 +45,9 @@ SIGNATURES = {
     "tfhe_keys_create": (ctypes.c_int, [ctypes.POINTER(TfheParams), _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "tfhe_keys_create_fourier": (ctypes.c_int, [ctypes.POINTER(TfheParams), _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "tfhe_keys_destroy": (None, [_P]),
+    "tfhe_keys_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TfheTuning)]),
+    "tfhe_keys_launch_shape": (ctypes.c_int, [_P, _I64, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                                              ctypes.POINTER(_I64)]),
     "tfhe_keys_device_bytes": (_I64, [_P]),
     "tfhe_keyswitch": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P]),
     "tfhe_blind_rotate": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _I64, _P]),

@@ -107,6 +107,20 @@ class Keys:
             raise RuntimeError("keys have been released")
         return self._h
 
+    def set_tuning(self, ciphertexts_per_cta=0, prefetch=-1, persistent=-1) -> None:
+        """Launch shape of this key set's blind rotations (speed only; 0 / -1
+        mean automatic).  tfhe_keys_set_tuning."""
+        t = _lib.TfheTuning(int(ciphertexts_per_cta), int(prefetch), int(persistent))
+        _lib.check(_lib.load().tfhe_keys_set_tuning(self.handle, ctypes.byref(t)))
+        self.tuning = (int(ciphertexts_per_cta), int(prefetch), int(persistent))
+
+    def launch_shape(self, batch: int):
+        """(ciphertexts per CTA, threads per CTA, shared bytes) a batch gets."""
+        k, nt, sm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        _lib.check(_lib.load().tfhe_keys_launch_shape(self.handle, int(batch), ctypes.byref(k), ctypes.byref(nt),
+                                                      ctypes.byref(sm)))
+        return k.value, nt.value, sm.value
+
     def device_bytes(self) -> int:
         return int(_lib.load().tfhe_keys_device_bytes(self.handle))
 
@@ -215,3 +229,40 @@ def probe_fp64_peak(iters=4096, reps=5) -> float:
         if i:
             best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
     return best
+
+
+class PBSGraph:
+    """One programmable bootstrap of a fixed batch captured in a CUDA graph:
+    the key switch and the blind rotation / extraction launches on fixed
+    device buffers, replayed per call (inputs are copied into the captured
+    buffers).  Removes the per-call host work of small batches."""
+
+    def __init__(self, keys: Keys, batch: int, n_lut: int = 1, lut_count: int = 1):
+        p = keys.params
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.keys, self.batch, self.n_lut = keys, batch, n_lut
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.a = torch.zeros((batch, p.big), **i32)
+        self.b = torch.zeros((batch,), **i32)
+        self.lut = torch.zeros((lut_count, 2, p.N), **i32)
+        self.ka = torch.empty((batch, p.n), **i32)
+        self.kb = torch.empty((batch,), **i32)
+        self.out_a = torch.empty((batch, n_lut, p.N), **i32)
+        self.out_b = torch.empty((batch, n_lut), **i32)
+        self._step()                      # uncaptured: sets kernel attributes
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._step()
+
+    def _step(self):
+        self.keys.keyswitch(self.a, self.b, self.ka, self.kb)
+        self.keys.cuboot_merge(self.ka, self.kb, self.lut, self.n_lut, self.out_a, self.out_b)
+
+    def __call__(self, a, b, lut=None):
+        self.a.copy_(a, non_blocking=True)
+        self.b.copy_(b, non_blocking=True)
+        if lut is not None:
+            self.lut.copy_(lut, non_blocking=True)
+        self.graph.replay()
+        return self.out_a, self.out_b

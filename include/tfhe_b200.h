@@ -52,6 +52,14 @@ typedef struct tfhe_params {
 
 typedef struct tfhe_keys tfhe_keys;   /* device-resident key material */
 
+/* Launch shape of the blind rotation for one key set (no counterpart in
+ * the reference; chosen by an autotuner or left automatic). */
+typedef struct tfhe_tuning {
+    int32_t ciphertexts_per_cta;  /* 0: as many as shared memory and 512 threads allow */
+    int32_t prefetch;             /* L1 prefetch of key words: -1 automatic, 0 off, 1 on */
+    int32_t persistent;           /* CTAs loop over ciphertext sets: -1 automatic (on), 0, 1 */
+} tfhe_tuning;
+
 /* library identification and the last error of the calling thread */
 const char* tfhe_version(void);
 const char* tfhe_last_error(void);
@@ -102,6 +110,13 @@ int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordere
                              void* stream, tfhe_keys** keys_out);
 
 void tfhe_keys_destroy(tfhe_keys* keys);
+
+/* Set (NULL: reset to automatic) the launch shape used by this key set's
+ * blind rotations, and query the shape a batch would get.  Tuning only
+ * changes speed, never results (no counterpart in the reference). */
+int tfhe_keys_set_tuning(tfhe_keys* keys, const tfhe_tuning* tuning);
+int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* ciphertexts_per_cta,
+                           int32_t* threads, int64_t* shared_bytes);
 int64_t tfhe_keys_device_bytes(const tfhe_keys* keys);
 
 /* Batched LWE key switch: key_switch_LWE vmapped over ciphertexts

@@ -350,3 +350,40 @@ def test_no_wait_timeouts_recorded():
     st = ctypes.c_int32()
     _lib.check(_lib.load().tfhe_device_status(ctypes.byref(st), 0))
     assert st.value == 0
+
+
+def test_tuning_changes_speed_not_results(tmp_path):
+    """Every launch shape gives identical outputs; the autotuner picks one,
+    caches it and the cache is applied on the next call."""
+    from tfhe_b200.autotune import autotune, candidates
+    name = "tiny_c3"
+    N = PARAMS[name]["N"]
+    eng = engine(name)
+    msgs, a, b = inputs(name, 21)
+    lut = device_u32(np.stack([np.zeros(N), step_body(name)])[None])
+    want = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+    for shape in candidates(eng, 21):
+        eng.set_tuning(*shape)
+        got = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), shape
+    path = str(tmp_path / "tune.json")
+    best, times = autotune(eng, 21, path=path, reps=1)
+    assert best in times
+    again, times2 = autotune(eng, 21, path=path)
+    assert again == best and times2 == {}
+    eng.set_tuning()                     # back to automatic for the other tests
+
+
+def test_cuda_graph_replay_matches_direct_calls():
+    from tfhe_b200.engine import PBSGraph
+    name = "tiny_c3"
+    N = PARAMS[name]["N"]
+    eng = engine(name)
+    lut = device_u32(np.stack([np.zeros(N), step_body(name)])[None])
+    graph = PBSGraph(eng, 13, n_lut=1)
+    for seed in (1, 2):
+        msgs, a, b = inputs(name, 13, seed_offset=seed)
+        want = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+        got = graph(device_u32(a), device_u32(b.reshape(-1)), lut)
+        torch.cuda.synchronize()
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
