@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample", type=int, default=96, help="ciphertexts in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep", default=None,
+                    help="comma-separated batch sizes: print one line per batch comparing the plain launch with "
+                         "the persistent, autotuned, CUDA-graph launch (one GPU)")
     return ap.parse_args()
 
 
@@ -273,6 +276,86 @@ def run_engine(args, rank, world, local_rank, dist):
     return line
 
 
+def run_sweep(args, batches):
+    """Batch sweep at the 2048 parameter set: for every batch size, the plain
+    launch (one CTA wave after another, automatic shape, direct calls) and
+    the persistent, autotuned launch replayed from a CUDA graph.  Both arms
+    time key switch + blind rotation + extraction on device-resident inputs
+    with CUDA events and decrypt every output."""
+    import numpy as np
+    import torch
+    from tfhe_b200 import client
+    from tfhe_b200.autotune import autotune
+    from tfhe_b200.engine import Keys, PBSGraph
+    from tfhe_b200.params import CONFIG2
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    p = CONFIG2
+    bmax = max(batches)
+    keys, msgs, a, b, lut, expect = make_inputs(p, bmax, args.seed)
+    eng = Keys.create(p, keys.bsk, keys.ksk_a, keys.ksk_b)
+    i32 = lambda x: torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).to(dev)
+    a_d, b_d, lut_d = i32(a), i32(b), i32(lut)
+    stream = torch.cuda.current_stream()
+    out = []
+    for B in batches:
+        steps = max(args.steps, min(200, 65536 // max(B, 1)))
+        ka = torch.empty((B, p.n), dtype=torch.int32, device=dev)
+        kb = torch.empty((B,), dtype=torch.int32, device=dev)
+        oa = torch.empty((B, 1, p.N), dtype=torch.int32, device=dev)
+        ob = torch.empty((B, 1), dtype=torch.int32, device=dev)
+
+        def timed(fn):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / steps
+
+        def errors(out_a, out_b):
+            dec = client.decrypt(out_a.cpu().numpy().view(np.uint32)[:, 0], out_b.cpu().numpy().view(np.uint32)[:, 0],
+                                 keys.sk_glwe, T_OUT)
+            return int(np.sum(dec != expect[:B]))
+
+        eng.set_tuning(0, -1, 0)
+
+        def plain():
+            eng.keyswitch(a_d[:B], b_d[:B], ka, kb)
+            eng.cuboot_merge(ka, kb, lut_d[:B], 1, oa, ob)
+
+        plain_ms = timed(plain)
+        plain_err = errors(oa, ob)
+        plain_shape = eng.launch_shape(B)
+
+        shape, _ = autotune(eng, B, use_cache=False, reps=2)
+        graph = PBSGraph(eng, B, n_lut=1, lut_count=B)
+        graph.lut.copy_(lut_d[:B])
+        graph.a.copy_(a_d[:B])
+        graph.b.copy_(b_d[:B])
+        tuned_ms = timed(graph.graph.replay)
+        tuned_err = errors(graph.out_a, graph.out_b)
+        same = bool(torch.equal(graph.out_a, oa) and torch.equal(graph.out_b, ob))
+        del graph
+        eng.set_tuning()
+        out.append({"sweep": "PBS+KS n=742 N=2048 gadget 2^15x2 KS 2^4x5 c=2", "batch": B, "steps": steps,
+                    "plain": {"ms_per_batch": round(plain_ms, 4), "PBS/s": round(B / plain_ms * 1e3, 1),
+                              "decrypt_errors": plain_err, "K": plain_shape[0], "persistent": 0},
+                    "persistent_autotuned_graph": {"ms_per_batch": round(tuned_ms, 4),
+                                                   "PBS/s": round(B / tuned_ms * 1e3, 1),
+                                                   "decrypt_errors": tuned_err,
+                                                   "shape": {"K": shape[0], "prefetch": shape[1],
+                                                             "persistent": shape[2]}},
+                    "outputs_equal": same, "speedup": round(plain_ms / tuned_ms, 3)})
+    eng.close()
+    return out
+
+
 def read_traffic(batch):
     """DRAM bytes per launch of the blind-rotation kernel from the committed
     ncu summary (bytes per ciphertext of a captured launch), or None."""
@@ -411,6 +494,11 @@ def main():
         _set_single_thread()
         line = run_reference(args, rank, world)
         if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+
+    if args.sweep:
+        for line in run_sweep(args, [int(x) for x in args.sweep.split(",")]):
             print(json.dumps(line), flush=True)
         return 0
 

@@ -165,3 +165,21 @@ def many_lut(N: int, n_lut: int, thresholds, s: float, t_out: int) -> np.ndarray
     # X^(-N/2) * full: coefficient k <- full[k + N/2], negated where it wraps
     rot = np.concatenate([full[N // 2:], -full[: N // 2]])
     return _u32(rot)
+
+
+def packed_table_lut(N: int, tables, t_out: int) -> np.ndarray:
+    """uint32 LUT body packing n_lut arbitrary tables f_i: Z_t -> Z_t_out
+    (inputs with a padding bit) for one blind rotation: sub-LUT i sits on
+    coefficients base * n_lut + i (the packing of nn_tfhe/utils_spike.py:72-87)
+    and holds f_i of the message decoded at position base * n_lut; after the
+    rotation by -b~ (a multiple of n_lut) coefficient i is f_i(m)."""
+    tables = np.asarray(tables, dtype=np.int64)
+    n_lut, t = tables.shape
+    box = N // t
+    pos = np.arange(0, N, n_lut)
+    m = (pos + box // 2) // box
+    scale = 1 << (32 - int(np.log2(t_out)))
+    body = np.zeros(N, dtype=np.int64)
+    for i in range(n_lut):
+        body[pos + i] = np.where(m < t, tables[i][np.minimum(m, t - 1)] * scale, -tables[i][0] * scale)
+    return _u32(body)
