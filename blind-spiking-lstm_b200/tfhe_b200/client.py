@@ -183,3 +183,56 @@ def packed_table_lut(N: int, tables, t_out: int) -> np.ndarray:
     for i in range(n_lut):
         body[pos + i] = np.where(m < t, tables[i][np.minimum(m, t - 1)] * scale, -tables[i][0] * scale)
     return _u32(body)
+
+
+# ---------------------------------------------------------------- RLWE level
+def encrypt_rlwe(msg, sk, sigma: float, rng):
+    """RLWE encryptions (schemas/RLWE_jax.py:36-54) of integer polynomials
+    msg (..., N) under the binary key sk (N,): (mask, body) uint32."""
+    return _glwe_encrypt(_u32(msg), np.asarray(sk), sigma, rng)
+
+
+def rlwe_phase(a, b, sk) -> np.ndarray:
+    """b - a * s on the torus, centred int64 (..., N)."""
+    prod = negacyclic_mul_binary(np.asarray(a, dtype=np.uint32), np.asarray(sk))
+    return _centred(_u32(_centred(b) - _centred(prod)))
+
+
+def automorphism(poly, k: int) -> np.ndarray:
+    """X -> X^k on integer polynomials (schemas/polynomial_jax.py:171-200)."""
+    poly = np.asarray(poly, dtype=np.int64)
+    N = poly.shape[-1]
+    idx = (np.arange(N) * k) % (2 * N)
+    out = np.zeros_like(poly)
+    out[..., idx % N] = np.where(idx >= N, -poly, poly)
+    return out
+
+
+def galois_keys(sk, log2_beta: int, l: int, sigma: float, rng) -> np.ndarray:
+    """Keys of pack_lwe_to_rlwe (get_galois_key, schemas/RLWE_jax.py:218-226):
+    for step i, k = 2^(log2 N - i) + 1, the RLWE key switching key
+    (get_keyswitch_sk, :91-98) from s(X^k) back to s: rows
+    RLWE_s(-s(X^k) q / beta^j), j = 1..l.  Returns uint32 (log2 N, l, 2, N)."""
+    sk = np.asarray(sk, dtype=np.int64)
+    N = sk.shape[-1]
+    steps = int(np.log2(N))
+    gj = (1 << (32 - np.arange(1, l + 1) * log2_beta)).astype(np.int64)
+    out = np.empty((steps, l, 2, N), dtype=np.uint32)
+    for i in range(steps):
+        s_auto = automorphism(sk, 2 ** (steps - i) + 1)
+        mask, body = encrypt_rlwe(-(gj[:, None] * s_auto[None, :]), sk, sigma, rng)
+        out[i, :, 0], out[i, :, 1] = mask, body
+    return out
+
+
+def packing_key(sk_lwe, sk_rlwe, log2_beta: int, l: int, sigma: float, rng) -> np.ndarray:
+    """Packing key (get_packing_KSK, schemas/RLWE_jax.py:205-215): for every
+    LWE key bit s_i and level j, RLWE_{sk_rlwe}(s_i q / beta^j) as a constant
+    polynomial.  Returns uint32 (n_dim, l, 2, N)."""
+    sk_lwe = np.asarray(sk_lwe, dtype=np.int64)
+    N = np.asarray(sk_rlwe).shape[-1]
+    gj = (1 << (32 - np.arange(1, l + 1) * log2_beta)).astype(np.int64)
+    msg = np.zeros((sk_lwe.shape[0], l, N), dtype=np.int64)
+    msg[:, :, 0] = sk_lwe[:, None] * gj[None, :]
+    mask, body = encrypt_rlwe(msg, sk_rlwe, sigma, rng)
+    return np.stack([mask, body], axis=2)

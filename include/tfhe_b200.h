@@ -212,6 +212,66 @@ int tfhe_probe_wait_timeout(int64_t limit_cycles, int32_t* waited_out);
 int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* scratch,
                         double* flops, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Spike-LSTM timestep operators (nn_tfhe/Spike_LSTM.py:15-62, 103-184).
+ * Integer plaintexts times ciphertexts are exact modulo 2^32; the reference
+ * rounds FP64 FFT products that are exact at these sizes.
+ * ---------------------------------------------------------------------- */
+
+/* Linear.__call__ (nn_tfhe/Spike_LSTM.py:48-58): for every ciphertext s and
+ * output j, W_j(X) * rlwe_s (multiply_plaintext_ciphertext), sample_extract
+ * at 0 (schemas/text_jax.py:191-208), + bias_j.
+ *   weights (J, N) int32 in the layout of Linear.set_weights (:28-41),
+ *   bias (J) int32, rlwe (S, 2, N) -> out_a (S, J, N), out_b (S, J). */
+int tfhe_linear_extract(const int32_t* weights, const int32_t* bias, int32_t J,
+                        const uint32_t* rlwe, int64_t S, int32_t N,
+                        uint32_t* out_a, uint32_t* out_b, void* stream);
+
+/* prepare_LUT's product (nn_tfhe/activation.py:103-106) summed over the
+ * packed sub-LUTs (nn_tfhe/Spike_LSTM.py:129-132):
+ *   out[s][k] = sum_{g < groups} luts[g][k](X) * rlwe[s][g][k]
+ *   luts (groups, per_group, N) int32, rlwe (S, groups, per_group, 2, N)
+ *   -> out (S, per_group, 2, N). */
+int tfhe_lut_mul_sum(const int32_t* luts, int32_t groups, int32_t per_group,
+                     const uint32_t* rlwe, int64_t S, int32_t N,
+                     uint32_t* out, void* stream);
+
+typedef struct tfhe_galois_keys tfhe_galois_keys;
+
+/* Galois keys of pack_lwe_to_rlwe (get_galois_key, schemas/RLWE_jax.py:
+ * 218-226): keys (log2 N, l, 2, N) uint32 on the device, step i switching
+ * from the automorphism X -> X^(2^(log2 N - i) + 1) of the secret back to
+ * it, l levels of base 2^log2_beta.  Converted once to the FP64 Fourier
+ * domain. */
+int tfhe_galois_keys_create(int32_t N, int32_t log2_beta, int32_t l, const uint32_t* keys,
+                            void* stream, tfhe_galois_keys** out);
+int tfhe_galois_keys_destroy(tfhe_galois_keys* keys);
+
+/* pack_lwe_to_rlwe (schemas/text_jax.py:316-345): modulus switch to q/N,
+ * trivial embedding, log2 N automorphism + key-switch trace steps.
+ *   lwe_a (R, N), lwe_b (R) -> out (R, 2, N), reduced modulo 2^32. */
+int tfhe_pack_lwe_to_rlwe(const tfhe_galois_keys* keys, const uint32_t* lwe_a,
+                          const uint32_t* lwe_b, int64_t R, uint32_t* out, void* stream);
+
+/* packing (schemas/text_jax.py:211-239): T LWEs of dimension n_dim per
+ * output into one RLWE of degree N with the packing key
+ * (get_packing_KSK, schemas/RLWE_jax.py:205-215) laid out as
+ * ksp (n_dim, l, 2, N) uint32.
+ *   lwe_a (S, T, n_dim), lwe_b (S, T) -> out (S, 2, N); T <= N, l <= 4. */
+int tfhe_pack_lwes(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
+                   const uint32_t* lwe_a, const uint32_t* lwe_b, int32_t T, int64_t S,
+                   uint32_t* out, void* stream);
+
+/* out[s] = X^rot * x[s] + y[s] for RLWEs (S, 2, N); y may be NULL
+ * (rotate_ciphertext, schemas/text_jax.py:348-362, and
+ * sum_ciphertext_ciphertext, :24-41).  out may alias y, and x only if
+ * rot == 0 mod 2N. */
+int tfhe_rlwe_rotate_add(const uint32_t* x, int32_t rot, const uint32_t* y, int64_t S,
+                         int32_t N, uint32_t* out, void* stream);
+
+/* out = x + y modulo 2^32 over n words (sums of LWE ciphertexts). */
+int tfhe_u32_add(const uint32_t* x, const uint32_t* y, int64_t n, uint32_t* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,171 @@
+"""Spike-LSTM operators on the GPU against the oracle, bit for bit: linear
++ extraction, pack_lwe_to_rlwe, LUT products, packing, rotation, and whole
+timesteps of CipherSpikeLSTM and the CipherMLP head."""
+import numpy as np
+import pytest
+import torch
+
+from lstm_cases import (GAL_L, GAL_LOG2_BETA, HIDDEN, INPUT_DIM, N_LUT, NAME, PK_L, PK_LOG2_BETA, cen,
+                        encrypt_inputs, layer_material)
+from oracle import lstm_oracle as LO
+from pbs_cases import PARAMS
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0) if torch.cuda.is_available() else None
+
+
+def d32(x):
+    return torch.from_numpy(np.ascontiguousarray((np.asarray(x, dtype=np.int64) & 0xFFFFFFFF).astype(np.uint32))
+                            .view(np.int32)).to(DEV)
+
+
+def h64(t):
+    return t.cpu().numpy().view(np.uint32).astype(np.int64)
+
+
+def u(x):
+    return np.asarray(x, dtype=np.int64) & 0xFFFFFFFF
+
+
+def rnd(rng, shape):
+    return rng.integers(0, 2 ** 32, size=shape, dtype=np.uint64).astype(np.int64) - 2 ** 31
+
+
+_DEV_LAYER = {}
+
+
+def device_layer():
+    if "x" in _DEV_LAYER:
+        return _DEV_LAYER["x"]
+    from tfhe_b200.engine import Keys
+    from tfhe_b200.lstm import CipherSpikeLSTM, GaloisKeys, LayerKeys, Linear
+    from tfhe_b200.params import TINY_C3
+    m = layer_material()
+    k = m["keys"]
+    pbs = Keys.create(TINY_C3, k.bsk_coeff, k.ksk[0], k.ksk[1].reshape(k.ksk[1].shape[:2]))
+    gk = GaloisKeys(m["galois"], GAL_LOG2_BETA, GAL_L, DEV)
+    ksp = torch.from_numpy(np.ascontiguousarray(m["ksp"]).view(np.int32)).to(DEV)
+    keys = LayerKeys(pbs, gk, ksp, PK_LOG2_BETA, PK_L)
+    N = PARAMS[NAME]["N"]
+    per = HIDDEN // N_LUT
+    lins = []
+    for g in "fio":
+        lin = Linear(per, N, 1.0, DEV)
+        lin.set_weights(m["mats"][g], m["biases"][g])
+        assert np.array_equal(lin.kernel_np, m["layer"][f"kern_{g}"])
+        lins.append(lin)
+    L = m["layer"]
+    layer = CipherSpikeLSTM(keys, INPUT_DIM, HIDDEN, N_LUT, *lins, L["lut_f"], L["lut_i"], L["lut_o"])
+    _DEV_LAYER["x"] = (m, keys, layer)
+    return _DEV_LAYER["x"]
+
+
+def test_linear_extract_matches_oracle():
+    from tfhe_b200.lstm import linear_extract
+    rng = np.random.default_rng(10)
+    N = 256
+    for J, S, density in ((5, 3, 0.05), (9, 2, 1.0)):
+        kern = rng.integers(-7, 8, size=(J, N)) * (rng.random((J, N)) < density)
+        bias = rng.integers(-2 ** 31, 2 ** 31, size=J)
+        ct = rnd(rng, (S, 2, N))
+        ga, gb = linear_extract(d32(kern), d32(bias), d32(ct))
+        for s in range(S):
+            wa, wb = LO.linear(kern, bias, (ct[s, 0], ct[s, 1]))
+            assert np.array_equal(h64(ga[s]), u(wa))
+            assert np.array_equal(h64(gb[s]), u(wb))
+
+
+@pytest.mark.parametrize("N,l,log2_beta", [(256, 6, 4), (512, 4, 6)])
+def test_pack_lwe_to_rlwe_matches_oracle(N, l, log2_beta):
+    from tfhe_b200 import client
+    from tfhe_b200.lstm import GaloisKeys
+    rng = np.random.default_rng(N + l)
+    sk = rng.integers(0, 2, size=N)
+    gal = client.galois_keys(sk, log2_beta, l, 1.0, rng)
+    gk = GaloisKeys(gal, log2_beta, l, DEV)
+    R = 5
+    a = rnd(rng, (R, N))
+    b = rnd(rng, (R,))
+    got = gk.pack_lwe_to_rlwe(d32(a), d32(b))
+    A, B = LO.pack_lwe_to_rlwe(a, b, cen(gal), log2_beta, l)
+    assert np.array_equal(h64(got[:, 0]), u(A))
+    assert np.array_equal(h64(got[:, 1]), u(B))
+    gk.close()
+
+
+def test_lut_mul_sum_matches_oracle():
+    from tfhe_b200.lstm import lut_mul_sum
+    rng = np.random.default_rng(11)
+    N, G, K, S = 256, 2, 3, 2
+    luts = rng.integers(-1, 2, size=(G, K, N)) * (rng.random((G, K, N)) < 0.3)
+    luts[0, 0] = rng.integers(-2 ** 20, 2 ** 20, size=N)            # a dense row with large values
+    ct = rnd(rng, (S, G, K, 2, N))
+    got = lut_mul_sum(d32(luts), d32(ct))
+    for s in range(S):
+        pa, pb = LO.multiply_plaintext_ciphertext(luts, (ct[s, :, :, 0], ct[s, :, :, 1]))
+        assert np.array_equal(h64(got[s, :, 0]), u(pa.sum(axis=0)))
+        assert np.array_equal(h64(got[s, :, 1]), u(pb.sum(axis=0)))
+
+
+@pytest.mark.parametrize("T", [1, 10, 256])
+def test_pack_lwes_matches_oracle(T):
+    from tfhe_b200.lstm import pack_lwes
+    m = layer_material()
+    rng = np.random.default_rng(12 + T)
+    N = 256
+    S = 2
+    a = rnd(rng, (S, T, N))
+    b = rnd(rng, (S, T))
+    ksp = torch.from_numpy(np.ascontiguousarray(m["ksp"]).view(np.int32)).to(DEV)
+    got = pack_lwes(ksp, PK_LOG2_BETA, PK_L, d32(a), d32(b))
+    for s in range(S):
+        pa, pb = LO.packing(a[s], b[s], m["layer"]["ksp_a"], m["layer"]["ksp_b"], PK_LOG2_BETA, PK_L, N)
+        assert np.array_equal(h64(got[s, 0]), u(pa))
+        assert np.array_equal(h64(got[s, 1]), u(pb))
+
+
+def test_rotate_add_matches_oracle():
+    from tfhe_b200.lstm import rlwe_rotate_add
+    rng = np.random.default_rng(13)
+    N, S = 256, 3
+    x = rnd(rng, (S, 2, N))
+    y = rnd(rng, (S, 2, N))
+    for rot in (0, 5, 255, 256, 300, 511, -7):
+        got = rlwe_rotate_add(d32(x), rot, d32(y))
+        for s in range(S):
+            ra, rb = LO.rotate((x[s, 0], x[s, 1]), rot)
+            assert np.array_equal(h64(got[s, 0]), u(ra + y[s, 0]))
+            assert np.array_equal(h64(got[s, 1]), u(rb + y[s, 1]))
+
+
+def test_spike_lstm_timesteps_match_oracle():
+    m, keys, layer = device_layer()
+    p = m["p"]
+    N = p["N"]
+    T, S = 2, 2
+    xs, _ = encrypt_inputs(m["sk"], T, S, N)
+    H = torch.zeros((S, 2, N), dtype=torch.int32, device=DEV)
+    C = torch.zeros_like(H)
+    oh = [(np.zeros(N, np.int64), np.zeros(N, np.int64)) for _ in range(S)]
+    oc = [(np.zeros(N, np.int64), np.zeros(N, np.int64)) for _ in range(S)]
+    for t in range(T):
+        H, C = layer.step(d32(xs[t]), H, C)
+        for s in range(S):
+            x_t = (cen(xs[t, s, 0]), cen(xs[t, s, 1]))
+            oh[s], oc[s] = LO.spike_lstm_step(m["keys"], p, m["layer"], x_t, oh[s], oc[s])
+            assert np.array_equal(h64(H[s, 0]), u(oh[s][0])), (t, s)
+            assert np.array_equal(h64(H[s, 1]), u(oh[s][1])), (t, s)
+            assert np.array_equal(h64(C[s, 0]), u(oc[s][0])), (t, s)
+            assert np.array_equal(h64(C[s, 1]), u(oc[s][1])), (t, s)
+
+
+def test_sequences_alone_equal_sequences_batched():
+    m, keys, layer = device_layer()
+    N = m["p"]["N"]
+    xs, _ = encrypt_inputs(m["sk"], 2, 3, N, seed=21)
+    xs_d = d32(xs)
+    (Hb, Cb), _ = layer(xs_d)
+    for s in range(3):
+        (Hs, Cs), _ = layer(xs_d[:, s:s + 1].contiguous())
+        assert torch.equal(Hs[0], Hb[s]) and torch.equal(Cs[0], Cb[s])
