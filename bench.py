@@ -47,6 +47,12 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample", type=int, default=96, help="ciphertexts in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lstm", action="store_true",
+                    help="one encrypted Spike-LSTM layer + head: sequences/s (one GPU)")
+    ap.add_argument("--seq-len", type=int, default=32)
+    ap.add_argument("--seqs", type=int, default=16)
+    ap.add_argument("--hidden", type=int, default=128)
+    ap.add_argument("--layers", type=int, default=1)
     ap.add_argument("--sweep", default=None,
                     help="comma-separated batch sizes: print one line per batch comparing the plain launch with "
                          "the persistent, autotuned, CUDA-graph launch (one GPU)")
@@ -276,6 +282,82 @@ def run_engine(args, rank, world, local_rank, dist):
     return line
 
 
+def run_lstm(args):
+    """Encrypted Spike-LSTM: token ids Zipf(1.1) over 8192, int embeddings
+    of dim 64 encrypted per timestep, hidden 128 (4 packed LUTs per
+    bootstrap), 3 gate linears with weights in [-7, 7], head linear + ReLU
+    bootstrap + packing + linear; `seqs` sequences of `seq_len` tokens per
+    step.  value: sequences/s with encrypted inputs resident on the GPU;
+    e2e: the same with the host -> device copy of every step's inputs and
+    the device -> host copy of the logits inside the timed region."""
+    import numpy as np
+    import torch
+    from tfhe_b200 import spike_model as SM
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    cfg = SM.SpikeModelConfig(hidden=args.hidden, layers=args.layers)
+    model = SM.build_model(cfg, args.seed)
+    dm = SM.to_device(model, dev)
+    rng = np.random.default_rng(args.seed + 5)
+    tokens = SM.sample_tokens(rng, args.seqs, args.seq_len, cfg.vocab, cfg.zipf)
+    xs_h = torch.from_numpy(SM.encrypt_tokens(model, tokens, rng).view(np.int32)).pin_memory()
+    xs_d = xs_h.to(dev)
+    stream = torch.cuda.current_stream()
+
+    def forward(xs):
+        H, _ = SM.run_layers(dm, xs)
+        return dm.head(H)
+
+    for _ in range(args.warmup):
+        forward(xs_d)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        la, lb = forward(xs_d)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+
+    la_h = torch.empty(la.shape, dtype=torch.int32).pin_memory()
+    lb_h = torch.empty(lb.shape, dtype=torch.int32).pin_memory()
+    xs_e = torch.empty_like(xs_d)
+    e0.record(stream)
+    for _ in range(args.steps):
+        xs_e.copy_(xs_h, non_blocking=True)
+        a, b = forward(xs_e)
+        la_h.copy_(a, non_blocking=True)
+        lb_h.copy_(b, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    logits = SM.decrypt_logits(model, la_h, lb_h)
+    plain, _ = SM.plain_forward(model, tokens)
+    per_step = 21 * cfg.layers
+    pbs_per_seq = args.seq_len * cfg.layers * 3 * (cfg.hidden // cfg.n_lut) + cfg.hidden
+    return {"metric": "encrypted Spike-LSTM sequences/s (layer + head)", "value": round(args.seqs / dev_ms * 1e3, 3),
+            "unit": "seq/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dev_ms, 2), "higher_is_better": True, "dtype": "u32 torus, f64 FFT",
+            "data": "synthetic: Zipf(1.1) tokens over 8192, random int weights / embeddings / thresholds",
+            "config": {"workload": "Spike-LSTM", "seqs": args.seqs, "seq_len": args.seq_len, "emb_dim": cfg.emb_dim,
+                       "hidden": cfg.hidden, "layers": cfg.layers, "n_lut": cfg.n_lut, "pbs": cfg.pbs.name,
+                       "weights": "[-7, 7]"},
+            "e2e": {"value": round(args.seqs / e2e_ms * 1e3, 3), "unit": "seq/s",
+                    "h2d_bytes_per_step": int(xs_h.numel() * 4), "d2h_bytes_per_step": int((la.numel() + lb.numel()) * 4)},
+            "pbs_per_sequence": pbs_per_seq, "pbs_per_s": round(pbs_per_seq * args.seqs / dev_ms * 1e3, 1),
+            "gpu_launches": args.steps * (per_step * args.seq_len + 6),
+            "decrypted_logits": [round(float(v), 2) for v in logits[:8]],
+            "plain_logits": [round(float(v), 2) for v in plain[:8]],
+            "logit_sign_agreement": float(np.mean(np.sign(logits) == np.sign(plain))),
+            "logit_mean_abs_diff": round(float(np.mean(np.abs(logits - plain))), 3),
+            "clocks": clk}
+
+
 def run_sweep(args, batches):
     """Batch sweep at the 2048 parameter set: for every batch size, the plain
     launch (one CTA wave after another, automatic shape, direct calls) and
@@ -495,6 +577,10 @@ def main():
         line = run_reference(args, rank, world)
         if line is not None:
             print(json.dumps(line), flush=True)
+        return 0
+
+    if args.lstm:
+        print(json.dumps(run_lstm(args)), flush=True)
         return 0
 
     if args.sweep:

@@ -244,3 +244,26 @@ def spike_lstm_step(keys, p, layer, x_t, H, C):
     H_t = packing(h_a, h_b, layer["ksp_a"], layer["ksp_b"], layer["pk_log2_beta"], layer["pk_l"], N)
     H_t = rotate(H_t, layer["input_dim"])
     return H_t, C_t
+
+
+def relu_lut(degree_lut, s, beta_x):
+    """ReluBoostrapper's LUT body (nn_tfhe/activation.py:186-194): a ramp
+    over the first N/2 coefficients (arange(0, s, 2s/N) * beta_x), zeros
+    after, rounded to integers for the uint32 torus."""
+    ramp = np.arange(degree_lut // 2) * (2.0 * s / degree_lut) * beta_x
+    return np.rint(np.concatenate([ramp, np.zeros(degree_lut // 2)])).astype(np.int64)
+
+
+def cipher_mlp(keys, p, head, H):
+    """CipherMLP.__call__ (nn_tfhe/Spike_LSTM.py:201-206) on one RLWE:
+    linear1, ReLU bootstrap per unit with n_lut = 1 (the reference's
+    `bootstrapping` rotates the LUT before the blind rotation, which equals
+    cuboot_merge's rotation after it in exact arithmetic), packing,
+    linear2.  Returns (a (J2, N), b (J2,))."""
+    h1_a, h1_b = linear(head["kern1"], head["bias1"], H)
+    J, N = h1_a.shape
+    luts_a = np.zeros((J, N), np.int64)
+    luts_b = np.asarray(head["relu_luts"], np.int64)
+    y_a, y_b = cuboot(keys, p, h1_a, h1_b, luts_a, luts_b, 1)
+    h2 = packing(y_a[:, 0], y_b[:, 0], head["ksp_a"], head["ksp_b"], head["pk_log2_beta"], head["pk_l"], N)
+    return linear(head["kern2"], head["bias2"], h2)

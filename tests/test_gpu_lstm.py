@@ -169,3 +169,30 @@ def test_sequences_alone_equal_sequences_batched():
     for s in range(3):
         (Hs, Cs), _ = layer(xs_d[:, s:s + 1].contiguous())
         assert torch.equal(Hs[0], Hb[s]) and torch.equal(Cs[0], Cb[s])
+
+
+def test_cipher_mlp_head_matches_oracle():
+    from tfhe_b200.lstm import CipherMLP, Linear
+    m, keys, layer = device_layer()
+    p = m["p"]
+    N = p["N"]
+    rng = np.random.default_rng(31)
+    W1 = rng.integers(-7, 8, size=(INPUT_DIM + HIDDEN, 6))
+    B1 = rng.integers(-2, 3, size=6) * 2 ** 22
+    W2 = rng.integers(-7, 8, size=(6, 1))
+    B2 = rng.integers(-2, 3, size=1) * 2 ** 22
+    lin1, lin2 = Linear(6, N, 1.0, DEV), Linear(1, N, 1.0, DEV)
+    lin1.set_weights(W1, B1)
+    lin2.set_weights(W2, B2)
+    s_head = rng.uniform(0.5, 2.0, size=6)
+    relu = np.stack([LO.relu_lut(N, s, 2.0 ** 22) for s in s_head])
+    head_dev = CipherMLP(keys, lin1, lin2, relu)
+    xs, _ = encrypt_inputs(m["sk"], 1, 2, N, seed=33)
+    got_a, got_b = head_dev(d32(xs[0]))
+    head = {"kern1": lin1.kernel_np, "bias1": lin1.bias_np, "kern2": lin2.kernel_np, "bias2": lin2.bias_np,
+            "relu_luts": relu, "ksp_a": m["layer"]["ksp_a"], "ksp_b": m["layer"]["ksp_b"],
+            "pk_log2_beta": PK_LOG2_BETA, "pk_l": PK_L}
+    for s in range(2):
+        wa, wb = LO.cipher_mlp(m["keys"], p, head, (cen(xs[0, s, 0]), cen(xs[0, s, 1])))
+        assert np.array_equal(h64(got_a[s]), u(wa))
+        assert np.array_equal(h64(got_b[s]), u(wb))
