@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--seqs", type=int, default=16)
     ap.add_argument("--hidden", type=int, default=128)
     ap.add_argument("--layers", type=int, default=1)
+    ap.add_argument("--serve", action="store_true",
+                    help="continuous-batching server with Poisson arrivals: p50/p99 latency and sequences/s")
+    ap.add_argument("--rate", type=float, default=2.0, help="requests per second (--serve)")
+    ap.add_argument("--requests", type=int, default=24, help="requests per serving run (--serve)")
+    ap.add_argument("--max-slots", type=int, default=64)
     ap.add_argument("--sweep", default=None,
                     help="comma-separated batch sizes: print one line per batch comparing the plain launch with "
                          "the persistent, autotuned, CUDA-graph launch (one GPU)")
@@ -358,6 +363,92 @@ def run_lstm(args):
             "clocks": clk}
 
 
+def run_serve(args):
+    """Serving: Poisson arrivals at --rate requests/s; each request an
+    encrypted sequence of U[8, 64] Zipf(1.1) tokens; 2-layer Spike-LSTM with
+    hidden 256 (layers and hidden from the flags when given), per-request
+    encrypted state kept on the GPU, continuous batching (every live
+    request's current timestep in one batched step).  Reports p50/p99
+    latency and sequences/s, next to the same requests served one at a time
+    (one slot: no batching across requests)."""
+    import numpy as np
+    import torch
+    from tfhe_b200 import spike_model as SM
+    from tfhe_b200.serving import DeviceStepModel, Request, SpikeLstmServer, latency_summary, run_arrivals, \
+        slots_for_memory
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    hidden = args.hidden if args.hidden != 128 else 256
+    layers = args.layers if args.layers != 1 else 2
+    cfg = SM.SpikeModelConfig(hidden=hidden, layers=layers)
+    model = SM.build_model(cfg, args.seed)
+    dm = SM.to_device(model, dev)
+    sm = DeviceStepModel(dm)
+    rng = np.random.default_rng(args.seed + 9)
+    t_max = 64
+    free, _ = torch.cuda.mem_get_info()
+    slots = slots_for_memory(sm, t_max, free, 16 << 30, args.max_slots)
+
+    def make_requests(n, rate):
+        gaps = rng.exponential(1.0 / rate, size=n)
+        arr = np.cumsum(gaps) - gaps[0]
+        out = []
+        for i in range(n):
+            T = int(rng.integers(8, 65))
+            tok = SM.sample_tokens(rng, 1, T, cfg.vocab, cfg.zipf)
+            xs = torch.from_numpy(SM.encrypt_tokens(model, tok, rng).view(np.int32))[:, 0].contiguous().pin_memory()
+            out.append(Request(i, xs, arrival=float(arr[i])))
+        return out
+
+    # warm-up: two short requests through a server
+    warm = SpikeLstmServer(sm, 2, t_max, dev)
+    for r in make_requests(2, 100.0):
+        r.xs = r.xs[:2].contiguous()
+        warm.submit(r)
+    for _ in range(max(1, args.warmup)):
+        warm.tick()
+    torch.cuda.synchronize()
+
+    reqs = make_requests(args.requests, args.rate)
+    clocks = ClockSampler(0)
+    clocks.start()
+    srv = SpikeLstmServer(sm, slots, t_max, dev)
+    done = run_arrivals(srv, reqs)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    span = max(r.done for r in done) - min(r.arrival for r in done)
+    lat = latency_summary(done)
+
+    # the same first few requests one at a time, back to back
+    k = min(6, len(reqs))
+    solo = SpikeLstmServer(sm, 1, t_max, dev)
+    import time as _t
+    t0 = _t.perf_counter()
+    solo_reqs = [Request(r.rid, r.xs, arrival=0.0) for r in reqs[:k]]
+    for r in solo_reqs:
+        r.arrival = _t.perf_counter()
+        solo.submit(r)
+        while not solo.idle():
+            solo.tick()
+    solo_span = _t.perf_counter() - t0
+    same = all(torch.equal(a.logits[0], b.logits[0]) and torch.equal(a.logits[1], b.logits[1])
+               for a, b in zip(solo_reqs, reqs[:k]))
+    tokens = sum(r.length for r in done)
+    return {"metric": "encrypted Spike-LSTM serving: p50/p99 latency and sequences/s", "value": round(len(done) / span, 3),
+            "unit": "seq/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32 torus, f64 FFT",
+            "data": "synthetic: Poisson arrivals, U[8,64] Zipf(1.1) tokens, random int weights",
+            "config": {"workload": "Spike-LSTM serving", "rate_req_per_s": args.rate, "requests": len(done),
+                       "layers": cfg.layers, "hidden": cfg.hidden, "emb_dim": cfg.emb_dim, "n_lut": cfg.n_lut,
+                       "slots": slots, "pbs": cfg.pbs.name},
+            "latency": {k2: (round(v, 3) if isinstance(v, float) else v) for k2, v in lat.items()},
+            "tokens_per_s": round(tokens / span, 2), "ticks": srv.ticks,
+            "mean_batch": round(float(np.mean(srv.batch_sizes)), 2), "max_batch": int(max(srv.batch_sizes)),
+            "one_at_a_time": {"requests": k, "seq_per_s": round(k / solo_span, 3),
+                              "results_equal_to_mix": bool(same)},
+            "clocks": clk}
+
+
 def run_sweep(args, batches):
     """Batch sweep at the 2048 parameter set: for every batch size, the plain
     launch (one CTA wave after another, automatic shape, direct calls) and
@@ -581,6 +672,10 @@ def main():
 
     if args.lstm:
         print(json.dumps(run_lstm(args)), flush=True)
+        return 0
+
+    if args.serve:
+        print(json.dumps(run_serve(args)), flush=True)
         return 0
 
     if args.sweep:
