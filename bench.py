@@ -213,22 +213,13 @@ def run_engine(args, rank, world, local_rank, dist):
     noise = ((noise + 2 ** 31) % 2 ** 32) - 2 ** 31
     noise_log2_std = float(np.log2(np.std(noise.astype(np.float64))))
 
-    # end to end through tfhe_pbs with host buffers
+    # end to end through tfhe_pbs_host with host buffers
     oa_h = torch.empty((B, 1, p.N), dtype=torch.int32).pin_memory()
     ob_h = torch.empty((B, 1), dtype=torch.int32).pin_memory()
-    a_e = torch.empty_like(a_d)
-    b_e = torch.empty_like(b_d)
-    lut_e = torch.empty_like(lut_d)
-    oa_e = torch.empty_like(oa)
-    ob_e = torch.empty_like(ob)
-
     def step_e2e():
-        a_e.copy_(a_h, non_blocking=True)
-        b_e.copy_(b_h, non_blocking=True)
-        lut_e.copy_(lut_h, non_blocking=True)
-        eng.pbs(a_e, b_e, lut_e, 1, oa_e, ob_e)
-        oa_h.copy_(oa_e, non_blocking=True)
-        ob_h.copy_(ob_e, non_blocking=True)
+        # tfhe_pbs_host: host buffers in and out, the uploads / downloads of
+        # each chunk overlapped with the compute of its neighbours
+        eng.pbs_host(a_h, b_h, lut_h, 1, oa_h, ob_h)
 
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -858,6 +859,112 @@ int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, 
     if (rc == TFHE_OK)
         rc = br_native(keys, ks, ks_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch, stream);
     const int rc2 = check_cuda(cudaFreeAsync(ks, stream), "cudaFreeAsync(key-switch output)");
+    return rc != TFHE_OK ? rc : rc2;
+}
+
+// tfhe_pbs from host buffers: the batch is cut into chunks; chunk i's
+// host -> device copy runs on its own stream while chunk i-1 computes on the
+// caller's stream and chunk i-2's outputs return on a third stream.  Two
+// device slots alternate; events order every reuse of a slot after the
+// work that last read it.
+int tfhe_pbs_host(const tfhe_keys* keys, const uint32_t* a_host, const uint32_t* b_host, const uint32_t* lut_host,
+                  int64_t lut_count, int32_t n_lut, uint32_t* out_a_host, uint32_t* out_b_host, int64_t batch,
+                  int64_t chunk, void* stream_v) {
+    TFHE_TRY(check_keys(keys));
+    if (batch < 0 || chunk < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch or chunk");
+    if (batch == 0) return TFHE_OK;
+    if (!a_host || !b_host || !lut_host || !out_a_host || !out_b_host)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (lut_count != 1 && lut_count != batch) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut_count must be 1 or batch");
+    if (n_lut < 1 || n_lut > keys->p.N) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut out of range");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    const tfhe_params& p = keys->p;
+    long long C = chunk > 0 ? chunk : std::max<long long>(2048, ((batch + 7) / 8 + 2047) / 2048 * 2048);
+    C = std::min<long long>(C, batch);
+    const size_t N = (size_t)p.N, nb = (size_t)p.n_big, n = (size_t)p.n;
+    const bool lut_per_ct = lut_count == batch && batch > 1;
+    const size_t lut_words = (lut_per_ct ? (size_t)C : 1) * 2 * N;
+    const size_t slot_words = (size_t)C * nb + C + lut_words + (size_t)C * (n + 1) + (size_t)C * n_lut * N +
+                              (size_t)C * n_lut;
+    uint32_t* scratch = nullptr;
+    TFHE_TRY(check_cuda(cudaMallocAsync(&scratch, 2 * slot_words * sizeof(uint32_t), stream),
+                        "cudaMallocAsync(host pipeline)"));
+    struct Slot {
+        uint32_t *a, *b, *lut, *ks, *oa, *ob;
+    } slot[2];
+    for (int s = 0; s < 2; ++s) {
+        uint32_t* base = scratch + s * slot_words;
+        slot[s].a = base;
+        slot[s].b = slot[s].a + (size_t)C * nb;
+        slot[s].lut = slot[s].b + C;
+        slot[s].ks = slot[s].lut + lut_words;
+        slot[s].oa = slot[s].ks + (size_t)C * (n + 1);
+        slot[s].ob = slot[s].oa + (size_t)C * n_lut * N;
+    }
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ready = nullptr, h2d_end = nullptr, d2h_end = nullptr;
+    cudaEvent_t h2d_done[2] = {}, comp_done[2] = {}, d2h_done[2] = {};
+    int rc = check_cuda(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (rc == TFHE_OK) rc = check_cuda(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t* e : {&ready, &h2d_end, &d2h_end, &h2d_done[0], &h2d_done[1], &comp_done[0], &comp_done[1],
+                           &d2h_done[0], &d2h_done[1]})
+        if (rc == TFHE_OK) rc = check_cuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+    if (rc == TFHE_OK) rc = check_cuda(cudaEventRecord(ready, stream), "event record");
+    if (rc == TFHE_OK) rc = check_cuda(cudaStreamWaitEvent(h2d, ready, 0), "stream wait");
+    if (rc == TFHE_OK) rc = check_cuda(cudaStreamWaitEvent(d2h, ready, 0), "stream wait");
+    if (rc == TFHE_OK && !lut_per_ct)
+        for (int s = 0; s < 2 && rc == TFHE_OK; ++s)
+            rc = check_cuda(cudaMemcpyAsync(slot[s].lut, lut_host, 2 * N * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                            h2d), "LUT upload");
+    const long long nchunks = (batch + C - 1) / C;
+    for (long long i = 0; i < nchunks && rc == TFHE_OK; ++i) {
+        const int s = (int)(i & 1);
+        const long long c0 = i * C;
+        const long long cb = std::min<long long>(C, batch - c0);
+        Slot& sl = slot[s];
+        if (i >= 2) rc = check_cuda(cudaStreamWaitEvent(h2d, comp_done[s], 0), "stream wait");
+        if (rc == TFHE_OK)
+            rc = check_cuda(cudaMemcpyAsync(sl.a, a_host + c0 * nb, (size_t)cb * nb * sizeof(uint32_t),
+                                            cudaMemcpyHostToDevice, h2d), "input upload");
+        if (rc == TFHE_OK)
+            rc = check_cuda(cudaMemcpyAsync(sl.b, b_host + c0, (size_t)cb * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                            h2d), "input upload");
+        if (rc == TFHE_OK && lut_per_ct)
+            rc = check_cuda(cudaMemcpyAsync(sl.lut, lut_host + (size_t)c0 * 2 * N, (size_t)cb * 2 * N * sizeof(uint32_t),
+                                            cudaMemcpyHostToDevice, h2d), "LUT upload");
+        if (rc == TFHE_OK) rc = check_cuda(cudaEventRecord(h2d_done[s], h2d), "event record");
+        if (rc == TFHE_OK) rc = check_cuda(cudaStreamWaitEvent(stream, h2d_done[s], 0), "stream wait");
+        if (rc == TFHE_OK && i >= 2) rc = check_cuda(cudaStreamWaitEvent(stream, d2h_done[s], 0), "stream wait");
+        uint32_t* ks_b = sl.ks + (size_t)cb * n;
+        if (rc == TFHE_OK) rc = launch_ks(keys, sl.a, sl.b, sl.ks, ks_b, cb, stream);
+        if (rc == TFHE_OK)
+            rc = br_native(keys, sl.ks, ks_b, sl.lut, lut_per_ct ? cb : 1, n_lut, nullptr, sl.oa, sl.ob, cb, stream);
+        if (rc == TFHE_OK) rc = check_cuda(cudaEventRecord(comp_done[s], stream), "event record");
+        if (rc == TFHE_OK) rc = check_cuda(cudaStreamWaitEvent(d2h, comp_done[s], 0), "stream wait");
+        if (rc == TFHE_OK)
+            rc = check_cuda(cudaMemcpyAsync(out_a_host + (size_t)c0 * n_lut * N, sl.oa,
+                                            (size_t)cb * n_lut * N * sizeof(uint32_t), cudaMemcpyDeviceToHost, d2h),
+                            "output download");
+        if (rc == TFHE_OK)
+            rc = check_cuda(cudaMemcpyAsync(out_b_host + (size_t)c0 * n_lut, sl.ob, (size_t)cb * n_lut * sizeof(uint32_t),
+                                            cudaMemcpyDeviceToHost, d2h), "output download");
+        if (rc == TFHE_OK) rc = check_cuda(cudaEventRecord(d2h_done[s], d2h), "event record");
+    }
+    // the caller's stream resumes after every copy; then the scratch is released
+    if (h2d && h2d_end) {
+        cudaEventRecord(h2d_end, h2d);
+        cudaStreamWaitEvent(stream, h2d_end, 0);
+    }
+    if (d2h && d2h_end) {
+        cudaEventRecord(d2h_end, d2h);
+        cudaStreamWaitEvent(stream, d2h_end, 0);
+    }
+    const int rc2 = check_cuda(cudaFreeAsync(scratch, stream), "cudaFreeAsync(host pipeline)");
+    for (cudaEvent_t e : {ready, h2d_end, d2h_end, h2d_done[0], h2d_done[1], comp_done[0], comp_done[1], d2h_done[0],
+                          d2h_done[1]})
+        if (e) cudaEventDestroy(e);
+    if (h2d) cudaStreamDestroy(h2d);
+    if (d2h) cudaStreamDestroy(d2h);
     return rc != TFHE_OK ? rc : rc2;
 }
 

@@ -59,6 +59,7 @@ SIGNATURES = {
     "tfhe_device_status": (ctypes.c_int, [ctypes.POINTER(_I32), _I32]),
     "tfhe_probe_wait_timeout": (ctypes.c_int, [_I64, ctypes.POINTER(_I32)]),
     "tfhe_keyswitch_ref": (ctypes.c_int, [_P, _P, _P, _P, _I32, _I32, _I32, _I32, _P, _P, _I64, _P]),
+    "tfhe_pbs_host": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _I64, _P]),
     "tfhe_linear_extract": (ctypes.c_int, [_P, _P, _I32, _P, _I64, _I32, _P, _P, _P]),
     "tfhe_lut_mul_sum": (ctypes.c_int, [_P, _I32, _I32, _P, _I64, _I32, _P, _P]),
     "tfhe_galois_keys_create": (ctypes.c_int, [_I32, _I32, _I32, _P, _P, ctypes.POINTER(_P)]),

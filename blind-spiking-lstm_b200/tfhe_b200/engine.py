@@ -107,6 +107,29 @@ class Keys:
             raise RuntimeError("keys have been released")
         return self._h
 
+    def pbs_host(self, a, b, lut, n_lut=1, out_a=None, out_b=None, chunk=0, stream=None):
+        """pbs from host (CPU, ideally pinned) tensors with the copies
+        overlapped chunk by chunk (tfhe_pbs_host); outputs are host tensors,
+        valid once the stream has synchronised."""
+        p = self.params
+        B = a.shape[0]
+        for t, name in ((a, "a"), (b, "b"), (lut, "lut")):
+            if t.device.type != "cpu" or t.dtype != torch.int32 or not t.is_contiguous():
+                raise ValueError(f"{name}: contiguous int32 host tensor required")
+        if tuple(a.shape) != (B, p.big) or tuple(b.shape) != (B,) or tuple(lut.shape[1:]) != (2, p.N):
+            raise ValueError("pbs_host: shapes (B, n_big), (B), (1|B, 2, N) required")
+        out_a = out_a if out_a is not None else torch.empty((B, n_lut, p.N), dtype=torch.int32).pin_memory()
+        out_b = out_b if out_b is not None else torch.empty((B, n_lut), dtype=torch.int32).pin_memory()
+        for t, name in ((out_a, "out_a"), (out_b, "out_b")):
+            if t.device.type != "cpu" or t.dtype != torch.int32 or not t.is_contiguous():
+                raise ValueError(f"{name}: contiguous int32 host tensor required")
+        if tuple(out_a.shape) != (B, n_lut, p.N) or tuple(out_b.shape) != (B, n_lut):
+            raise ValueError("pbs_host: outputs (B, n_lut, N), (B, n_lut) required")
+        _lib.check(_lib.load().tfhe_pbs_host(self.handle, a.data_ptr(), b.data_ptr(), lut.data_ptr(), lut.shape[0],
+                                             n_lut, out_a.data_ptr(), out_b.data_ptr(), B, int(chunk),
+                                             _stream(stream)))
+        return out_a, out_b
+
     def set_tuning(self, ciphertexts_per_cta=0, prefetch=-1, persistent=-1) -> None:
         """Launch shape of this key set's blind rotations (speed only; 0 / -1
         mean automatic).  tfhe_keys_set_tuning."""

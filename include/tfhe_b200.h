@@ -209,6 +209,17 @@ int tfhe_probe_wait_timeout(int64_t limit_cycles, int32_t* waited_out);
  * each running 8 independent FMA chains of `iters` steps; *flops receives
  * the flop count of the launch (host pointer); scratch is one device
  * double.  Time it with events on `stream`. */
+/* tfhe_pbs from HOST buffers (pinned, for overlap): the batch is processed
+ * in chunks of `chunk` ciphertexts (0: automatic); each chunk's upload,
+ * compute and download run on separate streams so the copies overlap the
+ * compute of neighbouring chunks.  Same layouts and results as tfhe_pbs
+ * (HeavysideBoostrapper.cuboot, nn_tfhe/activation.py:148-162); the
+ * caller's stream resumes after the last download. */
+int tfhe_pbs_host(const tfhe_keys* keys, const uint32_t* a_host, const uint32_t* b_host,
+                  const uint32_t* lut_host, int64_t lut_count, int32_t n_lut,
+                  uint32_t* out_a_host, uint32_t* out_b_host, int64_t batch, int64_t chunk,
+                  void* stream);
+
 int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* scratch,
                         double* flops, void* stream);
 

@@ -387,3 +387,23 @@ def test_cuda_graph_replay_matches_direct_calls():
         got = graph(device_u32(a), device_u32(b.reshape(-1)), lut)
         torch.cuda.synchronize()
         assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+
+
+@pytest.mark.parametrize("chunk,shared_lut", [(10, False), (10, True), (0, False), (37, True)])
+def test_pbs_from_host_buffers_matches_device_pbs(chunk, shared_lut):
+    """tfhe_pbs_host (chunked, copies overlapped) gives tfhe_pbs's outputs."""
+    name = "tiny_c3"
+    N = PARAMS[name]["N"]
+    eng = engine(name)
+    msgs, a, b = inputs(name, 37)
+    rng = np.random.default_rng(5)
+    luts = u32(np.stack([np.zeros((37, N)), rng.integers(0, 2 ** 32, size=(37, N))], axis=1))
+    if shared_lut:
+        luts = luts[:1]
+    a_h = torch.from_numpy(u32(a).view(np.int32)).pin_memory()
+    b_h = torch.from_numpy(u32(b.reshape(-1)).view(np.int32)).pin_memory()
+    lut_h = torch.from_numpy(np.ascontiguousarray(luts).view(np.int32)).pin_memory()
+    got_a, got_b = eng.pbs_host(a_h, b_h, lut_h, 2, chunk=chunk)
+    torch.cuda.synchronize()
+    want_a, want_b = eng.pbs(a_h.cuda(), b_h.cuda(), lut_h.cuda(), 2)
+    assert torch.equal(got_a, want_a.cpu()) and torch.equal(got_b, want_b.cpu())
