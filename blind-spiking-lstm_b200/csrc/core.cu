@@ -27,7 +27,9 @@ struct tfhe_keys {
     const tfhe::FftPlan* plan = nullptr;
     int64_t bytes = 0;
     int ring_kr = 0;            // > 0: key in the ring layout for K == ring_kr per CTA
-    tfhe_tuning tune = {0, -1, -1};   // launch shape of the blind rotation (0 / -1: automatic)
+    tfhe_tuning tune = {0, -1, -1, -1};   // launch shapes (0 / -1: automatic)
+    unsigned char* ksk_limbs = nullptr;  // int8 limbs of the key-switching key for the tensor cores
+    int ks_npad = 0;                     // limb rows (4 (n+1) rounded up to the CTA tile)
 };
 
 namespace tfhe {
@@ -448,6 +450,12 @@ static int launch_ks_key(const KsKey& key, int n_big, int n, int l, int log2_bet
 
 static int launch_ks(const tfhe_keys* k, const uint32_t* a_in, const uint32_t* b_in, uint32_t* a_out,
                      uint32_t* b_out, long long B, cudaStream_t stream) {
+    // the tensor-core kernel reads the input rows with 16-byte loads
+    if (k->ksk_limbs && k->tune.ks_tensor_cores != 0 && (reinterpret_cast<uintptr_t>(a_in) & 15) == 0) {
+        KsTcArgs args{a_in, b_in, k->ksk_limbs, k->p.n_big, k->p.n, k->p.l_ks, k->p.log2_beta_ks, k->ks_npad, B,
+                      a_out, b_out, WAIT_LIMIT_CYCLES, device_status_word()};
+        return launch_ks_tc(args, stream);
+    }
     const long long ldk = k->ldk, l = k->p.l_ks;
     const KsKey key{k->ksk, k->ksk + k->p.n, l * ldk, ldk, l * ldk, ldk};
     return launch_ks_key(key, k->p.n_big, k->p.n, k->p.l_ks, k->p.log2_beta_ks, a_in, b_in, a_out, b_out, B,
@@ -585,6 +593,31 @@ static int upload_ksk(tfhe_keys* k, const uint32_t* ksk_a, const uint32_t* ksk_b
     TFHE_TRY(check_cuda(cudaMalloc(&k->ksk, bytes), "cudaMalloc(ksk)"));
     k->bytes += (int64_t)bytes;
     TFHE_TRY(check_cuda(cudaMemcpyAsync(k->ksk, host.data(), bytes, cudaMemcpyHostToDevice, stream), "ksk upload"));
+    // int8 limbs for the tensor-core key switch, where its int32 sums cannot
+    // overflow: n_big * l * 2^(log2_beta - 1) * 128 < 2^31, digits within int8
+    const long long ktot = (long long)p.n_big * p.l_ks;
+    const bool tc_ok = p.n_big % 32 == 0 && p.l_ks <= 8 && p.log2_beta_ks <= 7 &&
+                       ktot * (1LL << (p.log2_beta_ks - 1)) * 128 < (1LL << 31);
+    if (tc_ok) {
+        const int cols = ks_tc_columns();
+        k->ks_npad = (4 * (p.n + 1) + cols - 1) / cols * cols;
+        std::vector<int8_t> lim((size_t)k->ks_npad * ktot, 0);
+        for (long long kk = 0; kk < ktot; ++kk)
+            for (int o = 0; o <= p.n; ++o) {
+                long long rest = host[(size_t)kk * k->ldk + o];
+                for (int t = 0; t < 4; ++t) {
+                    const long long lo = ((rest + 128) & 255) - 128;
+                    lim[((size_t)o * 4 + t) * ktot + kk] = (int8_t)lo;
+                    rest = (rest - lo) >> 8;
+                }
+            }
+        TFHE_TRY(check_cuda(cudaMalloc(&k->ksk_limbs, lim.size()), "cudaMalloc(ksk limbs)"));
+        k->bytes += (int64_t)lim.size();
+        TFHE_TRY(check_cuda(cudaMemcpyAsync(k->ksk_limbs, lim.data(), lim.size(), cudaMemcpyHostToDevice, stream),
+                            "ksk limb upload"));
+        // the host vector must outlive the copy
+        return check_cuda(cudaStreamSynchronize(stream), "ksk upload sync");
+    }
     return check_cuda(cudaStreamSynchronize(stream), "ksk upload sync");
 }
 
@@ -614,6 +647,7 @@ static void keys_free(tfhe_keys* k) {
     if (!k) return;
     cudaFree(k->bsk);
     cudaFree(k->ksk);
+    cudaFree(k->ksk_limbs);
     delete k;
 }
 
@@ -980,11 +1014,12 @@ int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* 
 int tfhe_keys_set_tuning(tfhe_keys* keys, const tfhe_tuning* tuning) {
     if (!keys) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys is NULL");
     if (!tuning) {
-        keys->tune = tfhe_tuning{0, -1, -1};
+        keys->tune = tfhe_tuning{0, -1, -1, -1};
         return TFHE_OK;
     }
     if (tuning->ciphertexts_per_cta < 0 || tuning->ciphertexts_per_cta > 64 || tuning->prefetch < -1 ||
-        tuning->prefetch > 1 || tuning->persistent < -1 || tuning->persistent > 1)
+        tuning->prefetch > 1 || tuning->persistent < -1 || tuning->persistent > 1 ||
+        tuning->ks_tensor_cores < -1 || tuning->ks_tensor_cores > 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "tuning out of range");
     keys->tune = *tuning;
     return TFHE_OK;

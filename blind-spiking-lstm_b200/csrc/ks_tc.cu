@@ -1,0 +1,235 @@
+// LWE key switching on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// key_switch_LWE (schemas/LWE_jax.py:97-117) is the integer contraction
+//   a'[o] = sum_k d[k] K[k][o],   b' = b + sum_k d[k] K[k][n],   k = i*l + j
+// of the gadget digits d (|d| <= 2^(log2_beta-1) <= 64, int8) of the input
+// mask with the key.  Every 32-bit key word is split into four signed 8-bit
+// limbs, K = sum_t limb_t 2^(8t) mod 2^32, so the contraction is four int8 x
+// int8 -> int32 GEMMs; their int32 sums cannot overflow (checked by the
+// launcher) and are recombined modulo 2^32 in the epilogue: bit-exact with
+// the integer key switch.
+//
+// Tile: 128 ciphertexts x 256 limb columns (64 outputs x 4 limbs) per CTA,
+// K in stages of 32 input coefficients (32*l digits).  Operands are staged
+// in shared memory in the canonical K-major no-swizzle layout (8-row x
+// 16-byte core matrices), two stages in flight; one thread issues
+// tcgen05.mma.kind::i8 (M=128, N=256, K=32) into a TMEM accumulator and
+// commits to an mbarrier per stage; the epilogue reads TMEM with tcgen05.ld.
+// Every mbarrier wait is bounded: on timeout the kernel records
+// TFHE_STATUS_WAIT_TIMEOUT and still releases its TMEM.
+#include <stdint.h>
+
+#include "tfhe_b200.h"
+#include "tfhe_dispatch.h"
+#include "tfhe_internal.cuh"
+
+namespace tfhe {
+
+namespace {
+
+constexpr int KTC_M = 128;          // ciphertexts per CTA (TMEM lanes)
+constexpr int KTC_N = 256;          // limb columns per CTA (TMEM columns)
+constexpr int KTC_COEF = 32;        // input coefficients per stage
+constexpr int KTC_THREADS = 256;
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// shared-memory matrix descriptor: K-major, no swizzle; lbo = byte distance
+// between the two 16-byte K chunks of one MMA, sbo = between 8-row groups
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    const uint32_t lo = ((saddr >> 4) & 0x3FFFu) | (((lbo >> 4) & 0x3FFFu) << 16);
+    const uint32_t hi = ((sbo >> 4) & 0x3FFFu) | (1u << 14);     // descriptor version 1, layout 0
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// instruction descriptor: D s32, A and B signed 8-bit, both K-major
+constexpr uint32_t KTC_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(KTC_N >> 3) << 17) |
+                               ((uint32_t)(KTC_M >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(KTC_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+template <int L>
+__global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_base_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int l = L;
+    constexpr int chunks = 2 * l;                        // 16-byte K chunks per row per stage
+    const uint32_t a_bytes = KTC_M * chunks * 16;    // one stage of A
+    const uint32_t b_bytes = KTC_N * chunks * 16;    // one stage of B
+    unsigned char* bufA[2] = {smem_raw, smem_raw + a_bytes + b_bytes};
+    unsigned char* bufB[2] = {smem_raw + a_bytes, smem_raw + 2 * a_bytes + b_bytes};
+    const uint32_t sbo = (uint32_t)chunks * 128;     // 8 rows x 16 bytes per core matrix
+    const long long row0 = (long long)blockIdx.y * KTC_M;
+    const int col0 = blockIdx.x * KTC_N;             // limb column (= 4 * output)
+    const int stages = a.n_big / KTC_COEF;
+    const long long kstride = (long long)a.n_big * l;   // bytes per key-limb row
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(&tmem_base_slot)),
+                     "r"((uint32_t)KTC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_slot;
+
+    const double inv_q = ldexp(1.0, -32);
+    const double beta = ldexp(1.0, a.log2_beta);
+    bool ok = true;
+
+    for (int s = 0; s < stages; ++s) {
+        const int buf = s & 1;
+        if (s >= 2)   // the MMAs of stage s - 2 have finished reading this buffer
+            ok &= mbar_wait_bounded(&bars[buf], (uint32_t)(((s - 2) >> 1) & 1), a.wait_limit, a.status);
+        // A: thread -> (row, half); 16 coefficients -> 16 l digits = l chunks
+        {
+            const int r = tid & (KTC_M - 1), half = tid >> 7;
+            const long long row = row0 + r;
+            const int i0 = s * KTC_COEF + half * 16;
+            int8_t dig[16 * L];
+            if (row < a.B) {
+                const uint4* src = reinterpret_cast<const uint4*>(a.a_in + row * a.n_big + i0);
+#pragma unroll
+                for (int q4 = 0; q4 < 4; ++q4) {
+                    const uint4 v = src[q4];
+                    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        double x = (double)(int32_t)w[e] * inv_q;
+#pragma unroll
+                        for (int j = 0; j < l; ++j) {
+                            const double y = x * beta;
+                            const double d = rint(y);
+                            x = y - d;
+                            dig[(q4 * 4 + e) * l + j] = (int8_t)(int)d;
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < 16 * l; ++t) dig[t] = 0;
+            }
+            unsigned char* base = bufA[buf] + (r >> 3) * sbo + (r & 7) * 16;
+#pragma unroll
+            for (int c = 0; c < l; ++c) {
+                uint4 v;
+                memcpy(&v, dig + c * 16, 16);
+                *reinterpret_cast<uint4*>(base + (half * l + c) * 128) = v;
+            }
+        }
+        // B: thread -> one limb row, 2 l chunks
+        {
+            const int r = tid;
+            const unsigned char* src = a.limbs + (long long)(col0 + r) * kstride + (long long)s * KTC_COEF * l;
+            unsigned char* base = bufB[buf] + (r >> 3) * sbo + (r & 7) * 16;
+#pragma unroll
+            for (int c = 0; c < chunks; ++c)
+                *reinterpret_cast<uint4*>(base + c * 128) = *reinterpret_cast<const uint4*>(src + c * 16);
+        }
+        fence_proxy_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sa = smem_addr(bufA[buf]), sb = smem_addr(bufB[buf]);
+            for (int kk = 0; kk < l; ++kk)     // K = 32 bytes = two chunks per MMA
+                mma_i8(tmem, smem_desc(sa + kk * 256, 128, sbo), smem_desc(sb + kk * 256, 128, sbo),
+                       (s > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(&bars[buf]);
+        }
+    }
+    // every issued MMA has completed once the last stage of each buffer has
+    for (int s = stages - 2; s < stages; ++s)
+        if (s >= 0) ok &= mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1), a.wait_limit, a.status);
+    tc_fence_after();
+
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) ..; warps 0-3 take limb
+    // columns 0-127, warps 4-7 columns 128-255
+    {
+        const int r = 32 * (warp & 3) + lane;
+        const long long row = row0 + r;
+        const int cbase = (warp >> 2) * (KTC_N / 2);
+        for (int c = cbase; c < cbase + KTC_N / 2; c += 8) {
+            uint32_t v[8];
+            tmem_ld8(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c, v);
+            tmem_wait_ld();
+            if (!ok || row >= a.B) continue;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o = (col0 + c) / 4 + h;
+                const uint32_t val = v[4 * h] + (v[4 * h + 1] << 8) + (v[4 * h + 2] << 16) + (v[4 * h + 3] << 24);
+                if (o < a.n) a.a_out[row * a.n + o] = val;
+                else if (o == a.n) a.b_out[row] = a.b_in[row] + val;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)KTC_N));
+}
+
+}  // namespace
+
+size_t ks_tc_smem_bytes(int l) { return (size_t)2 * (KTC_M + KTC_N) * 2 * l * 16; }
+
+int ks_tc_columns() { return KTC_N; }
+
+template <int L>
+static int launch_l(const KsTcArgs& args, cudaStream_t stream) {
+    const size_t smem = ks_tc_smem_bytes(L);
+    const cudaError_t e = cudaFuncSetAttribute(ks_tc_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "tensor-core key switch attribute");
+    const dim3 grid((unsigned)(args.npad / KTC_N), (unsigned)((args.B + KTC_M - 1) / KTC_M));
+    ks_tc_kernel<L><<<grid, KTC_THREADS, smem, stream>>>(args);
+    return check_cuda(cudaGetLastError(), "tensor-core key switch launch");
+}
+
+int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream) {
+    if (args.B == 0) return TFHE_OK;
+    if (args.npad % KTC_N || args.n_big % KTC_COEF || (args.B + KTC_M - 1) / KTC_M > 65535)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core key switch: unsupported shape");
+    switch (args.l) {
+        case 1: return launch_l<1>(args, stream);
+        case 2: return launch_l<2>(args, stream);
+        case 3: return launch_l<3>(args, stream);
+        case 4: return launch_l<4>(args, stream);
+        case 5: return launch_l<5>(args, stream);
+        case 6: return launch_l<6>(args, stream);
+        case 7: return launch_l<7>(args, stream);
+        case 8: return launch_l<8>(args, stream);
+        default: return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core key switch: 1 <= l <= 8");
+    }
+}
+
+}  // namespace tfhe

@@ -45,4 +45,20 @@ inline BrConvKernel bsk_fft_kernel_for(int logn) {
     }
 }
 
+// tensor-core LWE key switch (ks_tc.cu)
+struct KsTcArgs {
+    const uint32_t* a_in;         // (B, n_big)
+    const uint32_t* b_in;         // (B)
+    const unsigned char* limbs;   // (npad, n_big * l) int8: row 4 o + t = limb t of key column o
+    int n_big, n, l, log2_beta, npad;
+    long long B;
+    uint32_t* a_out;              // (B, n)
+    uint32_t* b_out;              // (B)
+    long long wait_limit;
+    int* status;
+};
+size_t ks_tc_smem_bytes(int l);
+int ks_tc_columns();
+int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream);
+
 }  // namespace tfhe

@@ -407,3 +407,38 @@ def test_pbs_from_host_buffers_matches_device_pbs(chunk, shared_lut):
     torch.cuda.synchronize()
     want_a, want_b = eng.pbs(a_h.cuda(), b_h.cuda(), lut_h.cuda(), 2)
     assert torch.equal(got_a, want_a.cpu()) and torch.equal(got_b, want_b.cpu())
+
+
+@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2", "c1_N128", "c4_N4096"])
+def test_keyswitch_tensor_cores_bit_exact(name):
+    """The tcgen05 int8 key switch equals the CUDA-core one and the oracle,
+    over partial and several 128-ciphertext tiles."""
+    k = keys(name)
+    eng = engine(name)
+    for batch in (37, 300):
+        msgs, a, b = inputs(name, batch, seed_offset=batch)
+        ra, rb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+        out = {}
+        for tc in (1, 0):
+            eng.set_tuning(ks_tensor_cores=tc)
+            out[tc] = eng.keyswitch(device_u32(a), device_u32(b.reshape(-1)))
+        eng.set_tuning()
+        assert torch.equal(out[1][0], out[0][0]) and torch.equal(out[1][1], out[0][1])
+        assert np.array_equal(host_u32(out[1][0]), u32(ra))
+        assert np.array_equal(host_u32(out[1][1]), u32(rb.reshape(-1)))
+
+
+def test_keyswitch_unaligned_input_uses_cuda_cores():
+    """An input not 16-byte aligned takes the CUDA-core kernel (the
+    tensor-core kernel loads 16-byte vectors) and is still exact."""
+    name = "tiny_c3"
+    k = keys(name)
+    eng = engine(name)
+    msgs, a, b = inputs(name, 9)
+    big = torch.zeros((9 * a.shape[1] + 1,), dtype=torch.int32, device="cuda")
+    big[1:] = device_u32(a).reshape(-1)
+    a_view = big[1:].view(9, a.shape[1])
+    assert a_view.data_ptr() % 16 != 0
+    ga, gb = eng.keyswitch(a_view, device_u32(b.reshape(-1)))
+    ra, rb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
+    assert np.array_equal(host_u32(ga), u32(ra)) and np.array_equal(host_u32(gb), u32(rb.reshape(-1)))
