@@ -310,7 +310,7 @@ __device__ __forceinline__ void stage_all(double2* polys, int npoly, const doubl
 }
 
 // ----------------------------------------------------------------------------
-// asynchronous bulk copies (TMA, 1D, no multicast) and mbarriers
+// asynchronous 1D bulk copies into this CTA's own shared memory, and mbarriers
 // ----------------------------------------------------------------------------
 // device status word values (tfhe_device_status)
 constexpr int TFHE_STATUS_WAIT_TIMEOUT = 1;
