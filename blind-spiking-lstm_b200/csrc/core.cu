@@ -130,7 +130,7 @@ static std::map<std::pair<int, int>, FftPlan*> g_plans;   // (device, N)
 static std::map<int, int*> g_status;                      // device -> status word
 
 // the device status word kernels write on a bounded-wait timeout
-static int* device_status_word() {
+int* device_status_word() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
     std::lock_guard<std::mutex> lk(g_plan_mu);
@@ -217,7 +217,6 @@ struct BrShape {
 };
 
 // a mbarrier wait gives up after this many cycles (about 2 s)
-constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL;
 
 // ciphertexts per CTA: as many as 512 threads and shared memory allow, or
 // TFHE_B200_K (tuning: K = 1 lets two CTAs share an SM)
@@ -453,7 +452,7 @@ static int launch_ks(const tfhe_keys* k, const uint32_t* a_in, const uint32_t* b
     // the tensor-core kernel reads the input rows with 16-byte loads
     if (k->ksk_limbs && k->tune.ks_tensor_cores != 0 && (reinterpret_cast<uintptr_t>(a_in) & 15) == 0) {
         KsTcArgs args{a_in, b_in, k->ksk_limbs, k->p.n_big, k->p.n, k->p.l_ks, k->p.log2_beta_ks, k->ks_npad, B,
-                      a_out, b_out, WAIT_LIMIT_CYCLES, device_status_word()};
+                      a_out, b_out, WAIT_LIMIT_CYCLES, device_status_word(), 0, 0, nullptr};
         return launch_ks_tc(args, stream);
     }
     const long long ldk = k->ldk, l = k->p.l_ks;

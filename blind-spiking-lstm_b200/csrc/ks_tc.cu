@@ -19,6 +19,8 @@
 // TFHE_STATUS_WAIT_TIMEOUT and still releases its TMEM.
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "tfhe_b200.h"
 #include "tfhe_dispatch.h"
 #include "tfhe_internal.cuh"
@@ -70,7 +72,7 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-template <int L>
+template <int L, bool PACK>
 __global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -189,8 +191,22 @@ __global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
             for (int h = 0; h < 2; ++h) {
                 const int o = (col0 + c) / 4 + h;
                 const uint32_t val = v[4 * h] + (v[4 * h + 1] << 8) + (v[4 * h + 2] << 16) + (v[4 * h + 3] << 24);
-                if (o < a.n) a.a_out[row * a.n + o] = val;
-                else if (o == a.n) a.b_out[row] = a.b_in[row] + val;
+                if constexpr (PACK) {
+                    if (o >= 2 * a.pack_N) continue;
+                    const long long sq = row / a.pack_T;
+                    const int t = (int)(row - sq * a.pack_T);
+                    const int poly = o / a.pack_N, cc = o - poly * a.pack_N;
+                    int d = cc + t;
+                    uint32_t add = 0u - val;               // -X^t V: negated unless it wraps past X^N
+                    if (d >= a.pack_N) {
+                        d -= a.pack_N;
+                        add = val;
+                    }
+                    atomicAdd(a.pack_out + (sq * 2 + poly) * (long long)a.pack_N + d, add);
+                } else {
+                    if (o < a.n) a.a_out[row * a.n + o] = val;
+                    else if (o == a.n) a.b_out[row] = a.b_in[row] + val;
+                }
             }
         }
     }
@@ -205,31 +221,69 @@ size_t ks_tc_smem_bytes(int l) { return (size_t)2 * (KTC_M + KTC_N) * 2 * l * 16
 
 int ks_tc_columns() { return KTC_N; }
 
-template <int L>
+template <int L, bool PACK>
 static int launch_l(const KsTcArgs& args, cudaStream_t stream) {
     const size_t smem = ks_tc_smem_bytes(L);
-    const cudaError_t e = cudaFuncSetAttribute(ks_tc_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "tensor-core key switch attribute");
+    const cudaError_t e =
+        cudaFuncSetAttribute(ks_tc_kernel<L, PACK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "tensor-core contraction attribute");
     const dim3 grid((unsigned)(args.npad / KTC_N), (unsigned)((args.B + KTC_M - 1) / KTC_M));
-    ks_tc_kernel<L><<<grid, KTC_THREADS, smem, stream>>>(args);
-    return check_cuda(cudaGetLastError(), "tensor-core key switch launch");
+    ks_tc_kernel<L, PACK><<<grid, KTC_THREADS, smem, stream>>>(args);
+    return check_cuda(cudaGetLastError(), "tensor-core contraction launch");
+}
+
+template <bool PACK>
+static int launch_any(const KsTcArgs& args, cudaStream_t stream) {
+    switch (args.l) {
+        case 1: return launch_l<1, PACK>(args, stream);
+        case 2: return launch_l<2, PACK>(args, stream);
+        case 3: return launch_l<3, PACK>(args, stream);
+        case 4: return launch_l<4, PACK>(args, stream);
+        case 5: return launch_l<5, PACK>(args, stream);
+        case 6: return launch_l<6, PACK>(args, stream);
+        case 7: return launch_l<7, PACK>(args, stream);
+        case 8: return launch_l<8, PACK>(args, stream);
+        default: return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core contraction: 1 <= l <= 8");
+    }
 }
 
 int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream) {
     if (args.B == 0) return TFHE_OK;
     if (args.npad % KTC_N || args.n_big % KTC_COEF || (args.B + KTC_M - 1) / KTC_M > 65535)
-        return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core key switch: unsupported shape");
-    switch (args.l) {
-        case 1: return launch_l<1>(args, stream);
-        case 2: return launch_l<2>(args, stream);
-        case 3: return launch_l<3>(args, stream);
-        case 4: return launch_l<4>(args, stream);
-        case 5: return launch_l<5>(args, stream);
-        case 6: return launch_l<6>(args, stream);
-        case 7: return launch_l<7>(args, stream);
-        case 8: return launch_l<8>(args, stream);
-        default: return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core key switch: 1 <= l <= 8");
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core contraction: unsupported shape");
+    if (args.pack_T > 0) {
+        if (!args.pack_out || args.npad != 8 * args.pack_N)
+            return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core packing: bad arguments");
+        return launch_any<true>(args, stream);
     }
+    return launch_any<false>(args, stream);
+}
+
+// limb rows of a packing key: row 4 o + t, o = poly * N + c, column k = i l + j
+// holds limb t of ksp[i][j][poly][c]
+__global__ void packing_limbs_kernel(const uint32_t* __restrict__ ksp, int n_dim, int l, int N,
+                                     int8_t* __restrict__ limbs) {
+    const long long K = (long long)n_dim * l;
+    const long long total = 2LL * N * K;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long o = idx / K;
+        const long long k = idx - o * K;
+        const int poly = (int)(o / N), c = (int)(o - (long long)poly * N);
+        long long rest = ksp[(k * 2 + poly) * N + c];
+        for (int t = 0; t < 4; ++t) {
+            const long long lo = ((rest + 128) & 255) - 128;
+            limbs[(o * 4 + t) * K + k] = (int8_t)lo;
+            rest = (rest - lo) >> 8;
+        }
+    }
+}
+
+int build_packing_limbs(const uint32_t* ksp, int n_dim, int l, int N, int8_t* limbs, cudaStream_t stream) {
+    const long long total = 2LL * N * n_dim * l;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+    packing_limbs_kernel<<<blocks, 256, 0, stream>>>(ksp, n_dim, l, N, limbs);
+    return check_cuda(cudaGetLastError(), "packing limb launch");
 }
 
 }  // namespace tfhe

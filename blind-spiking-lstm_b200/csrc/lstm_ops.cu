@@ -20,6 +20,7 @@
 #include <string>
 
 #include "tfhe_b200.h"
+#include "tfhe_dispatch.h"
 #include "tfhe_internal.cuh"
 
 namespace tfhe {
@@ -461,6 +462,12 @@ static int grid_for(long long total) {
 // ================================================================ C ABI
 using namespace tfhe;
 
+struct tfhe_packing_key {
+    int n_dim = 0, N = 0, log2_beta = 0, l = 0, device = 0;
+    uint32_t* ksp = nullptr;        // (n_dim, l, 2, N)
+    int8_t* limbs = nullptr;        // (8 N, n_dim l) int8 limbs for the tensor cores, or null
+};
+
 struct tfhe_galois_keys {
     int N = 0, log2_beta = 0, l = 0, steps = 0, device = 0;
     double2* key = nullptr;     // [steps][l][2][H]
@@ -638,6 +645,74 @@ int tfhe_pack_lwes(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_b
     const dim3 grid((2 * N + PK_TO - 1) / PK_TO, (unsigned)((rows + PK_TB - 1) / PK_TB));
     pack_ks_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(lwe_a, n_dim, T, S, ksp, N, l, log2_beta, out);
     return check_cuda(cudaGetLastError(), "packing launch");
+}
+
+int tfhe_packing_key_create(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
+                            void* stream, tfhe_packing_key** out) {
+    if (!out) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing key: null output");
+    *out = nullptr;
+    if (!valid_degree(N)) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing key: N must be a power of two in [128, 4096]");
+    if (l < 1 || l > PK_LMAX || log2_beta < 1 || log2_beta * l > 32 || n_dim < 1)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "packing key: need n_dim >= 1, 1 <= l <= 4, l * log2_beta <= 32");
+    if (!ksp) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing key: null key");
+    cudaStream_t st = (cudaStream_t)stream;
+    auto* k = new tfhe_packing_key();
+    k->n_dim = n_dim;
+    k->N = N;
+    k->log2_beta = log2_beta;
+    k->l = l;
+    cudaGetDevice(&k->device);
+    const size_t words = (size_t)n_dim * l * 2 * N;
+    int rc = check_cuda(cudaMalloc(&k->ksp, words * sizeof(uint32_t)), "cudaMalloc(packing key)");
+    if (rc == TFHE_OK)
+        rc = check_cuda(cudaMemcpyAsync(k->ksp, ksp, words * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
+                        "packing key copy");
+    // int8 limbs where the digits fit int8 and the int32 sums cannot overflow
+    const long long K = (long long)n_dim * l;
+    const bool tc = log2_beta <= 7 && n_dim % 32 == 0 && K * (1LL << (log2_beta - 1)) * 128 < (1LL << 31) &&
+                    (8 * N) % ks_tc_columns() == 0;
+    if (rc == TFHE_OK && tc) {
+        rc = check_cuda(cudaMalloc(&k->limbs, (size_t)8 * N * K), "cudaMalloc(packing limbs)");
+        if (rc == TFHE_OK) rc = build_packing_limbs(k->ksp, n_dim, l, N, k->limbs, st);
+    }
+    if (rc == TFHE_OK) rc = check_cuda(cudaStreamSynchronize(st), "packing key upload");
+    if (rc != TFHE_OK) {
+        cudaFree(k->ksp);
+        cudaFree(k->limbs);
+        delete k;
+        return rc;
+    }
+    *out = k;
+    return TFHE_OK;
+}
+
+int tfhe_packing_key_destroy(tfhe_packing_key* key) {
+    if (!key) return TFHE_OK;
+    cudaFree(key->ksp);
+    cudaFree(key->limbs);
+    delete key;
+    return TFHE_OK;
+}
+
+int tfhe_packing_key_uses_tensor_cores(const tfhe_packing_key* key) { return key && key->limbs ? 1 : 0; }
+
+int tfhe_pack_lwes_with_key(const tfhe_packing_key* key, const uint32_t* lwe_a, const uint32_t* lwe_b, int32_t T,
+                            int64_t S, uint32_t* out, int32_t tensor_cores, void* stream) {
+    if (!key) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: null key");
+    if (tensor_cores < -1 || tensor_cores > 1) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: tensor_cores in {-1, 0, 1}");
+    const int N = key->N;
+    const bool tc = key->limbs && tensor_cores != 0 && T > 0 && (reinterpret_cast<uintptr_t>(lwe_a) & 15) == 0;
+    if (!tc) return tfhe_pack_lwes(key->ksp, key->n_dim, N, key->log2_beta, key->l, lwe_a, lwe_b, T, S, out, stream);
+    if (T > N || S < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: bad sizes (T <= N)");
+    if (S == 0) return TFHE_OK;
+    if (!lwe_a || !lwe_b || !out) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: null pointer");
+    const long long total = S * 2 * (long long)N;
+    pack_init_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(lwe_b, T, S, N, out);
+    const int rc = check_cuda(cudaGetLastError(), "packing init launch");
+    if (rc != TFHE_OK) return rc;
+    KsTcArgs a{lwe_a, nullptr, reinterpret_cast<const unsigned char*>(key->limbs), key->n_dim, 0, key->l,
+               key->log2_beta, 8 * N, S * T, nullptr, nullptr, WAIT_LIMIT_CYCLES, device_status_word(), T, N, out};
+    return launch_ks_tc(a, (cudaStream_t)stream);
 }
 
 int tfhe_rlwe_rotate_add(const uint32_t* x, int32_t rot, const uint32_t* y, int64_t S, int32_t N, uint32_t* out,

@@ -56,9 +56,14 @@ struct KsTcArgs {
     uint32_t* b_out;              // (B)
     long long wait_limit;
     int* status;
+    // packing epilogue (pack_T > 0): row s*T + t adds -X^t V into RLWE s of
+    // pack_out (S, 2, pack_N); limb row 4 o + t with o = poly * N + coefficient
+    int pack_T, pack_N;
+    uint32_t* pack_out;
 };
 size_t ks_tc_smem_bytes(int l);
 int ks_tc_columns();
 int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream);
+int build_packing_limbs(const uint32_t* ksp, int n_dim, int l, int N, int8_t* limbs, cudaStream_t stream);
 
 }  // namespace tfhe

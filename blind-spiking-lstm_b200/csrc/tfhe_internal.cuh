@@ -25,6 +25,10 @@ namespace tfhe {
 // status handling shared by the C entry points
 // ----------------------------------------------------------------------------
 void set_error(const std::string& msg);
+// the per-device word kernels set on a bounded-wait timeout (tfhe_device_status)
+int* device_status_word();
+// bound of every mbarrier wait, in clock cycles (about 2 s)
+constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL;
 int fail(int code, const std::string& msg);
 int check_cuda(cudaError_t e, const char* what);
 

@@ -66,6 +66,10 @@ SIGNATURES = {
     "tfhe_galois_keys_destroy": (ctypes.c_int, [_P]),
     "tfhe_pack_lwe_to_rlwe": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P]),
     "tfhe_pack_lwes": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _I32, _I64, _P, _P]),
+    "tfhe_packing_key_create": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, ctypes.POINTER(_P)]),
+    "tfhe_packing_key_destroy": (ctypes.c_int, [_P]),
+    "tfhe_packing_key_uses_tensor_cores": (ctypes.c_int, [_P]),
+    "tfhe_pack_lwes_with_key": (ctypes.c_int, [_P, _P, _P, _I32, _I64, _P, _I32, _P]),
     "tfhe_rlwe_rotate_add": (ctypes.c_int, [_P, _I32, _P, _I64, _I32, _P, _P]),
     "tfhe_u32_add": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "tfhe_rotate_extract_i64": (ctypes.c_int, [_P, _P, _I32, _I32, _I64, _P, _P, _P, _I64, _P]),

@@ -109,6 +109,48 @@ def pack_lwes(ksp, log2_beta, l, lwe_a, lwe_b, out=None, stream=None):
     return out
 
 
+class PackingKey:
+    """Device packing key (tfhe_packing_key_create): packs T LWEs per RLWE on
+    the tcgen05 tensor cores where the key allows, else on CUDA cores."""
+
+    def __init__(self, ksp_u32: np.ndarray, log2_beta: int, l: int, device=None, stream=None):
+        n_dim, l2, two, N = ksp_u32.shape
+        if l2 != l or two != 2:
+            raise ValueError("packing key must be (n_dim, l, 2, N)")
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        src = torch.from_numpy(np.ascontiguousarray(ksp_u32).view(np.int32)).to(dev)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().tfhe_packing_key_create(_ptr(src), n_dim, N, log2_beta, l, _stream(stream),
+                                                       ctypes.byref(h)))
+        self._h, self.n_dim, self.N, self.log2_beta, self.l = h, n_dim, N, log2_beta, l
+
+    @property
+    def tensor_cores(self) -> bool:
+        return bool(_lib.load().tfhe_packing_key_uses_tensor_cores(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.load().tfhe_packing_key_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pack(self, lwe_a, lwe_b, out=None, tensor_cores=-1, stream=None):
+        """lwe_a (S, T, n_dim), lwe_b (S, T) -> (S, 2, N)."""
+        S, T, nd = lwe_a.shape
+        _need(lwe_a, torch.int32, (S, T, self.n_dim), "lwe_a")
+        _need(lwe_b, torch.int32, (S, T), "lwe_b")
+        out = out if out is not None else torch.empty((S, 2, self.N), dtype=torch.int32, device=lwe_a.device)
+        _need(out, torch.int32, (S, 2, self.N), "out")
+        _lib.check(_lib.load().tfhe_pack_lwes_with_key(self._h, _ptr(lwe_a), _ptr(lwe_b), T, S, _ptr(out),
+                                                       int(tensor_cores), _stream(stream)))
+        return out
+
+
 def rlwe_rotate_add(x, rot, y=None, out=None, stream=None):
     """X^rot * x + y for RLWEs (S, 2, N)."""
     S, two, N = x.shape
@@ -179,6 +221,12 @@ class LayerKeys:
     ksp: torch.Tensor         # packing key (N, l, 2, N) int32
     pk_log2_beta: int
     pk_l: int
+    packing: "PackingKey" = None   # device packing key (tensor cores where possible)
+
+    def pack(self, lwe_a, lwe_b, stream=None):
+        if self.packing is not None:
+            return self.packing.pack(lwe_a, lwe_b, stream=stream)
+        return pack_lwes(self.ksp, self.pk_log2_beta, self.pk_l, lwe_a, lwe_b, stream=stream)
 
 
 class CipherSpikeLSTM:
@@ -247,8 +295,8 @@ class CipherSpikeLSTM:
                                      lut_h.reshape(S * per, 2, N), self.n_lut, stream=stream)
         h_a, h_b = self._spikes(h_a, h_b, S)
         k = self.keys
-        C_t = pack_lwes(k.ksp, k.pk_log2_beta, k.pk_l, ct_a, ct_b, stream=stream)
-        H_p = pack_lwes(k.ksp, k.pk_log2_beta, k.pk_l, h_a, h_b, stream=stream)
+        C_t = k.pack(ct_a, ct_b, stream=stream)
+        H_p = k.pack(h_a, h_b, stream=stream)
         H_t = rlwe_rotate_add(H_p, self.input_dim, stream=stream)
         return H_t, C_t
 
@@ -285,5 +333,5 @@ class CipherMLP:
         y_a, y_b = self.keys.pbs.pbs(h1_a.reshape(S * J, N), h1_b.reshape(S * J), luts.reshape(S * J, 2, N), 1,
                                      stream=stream)
         k = self.keys
-        h2 = pack_lwes(k.ksp, k.pk_log2_beta, k.pk_l, y_a.reshape(S, J, N), y_b.reshape(S, J), stream=stream)
+        h2 = k.pack(y_a.reshape(S, J, N), y_b.reshape(S, J), stream=stream)
         return self.linear2(h2, stream)

@@ -19,7 +19,7 @@ import torch
 
 from . import client
 from .engine import Keys
-from .lstm import CipherMLP, CipherSpikeLSTM, GaloisKeys, LayerKeys, Linear
+from .lstm import CipherMLP, CipherSpikeLSTM, GaloisKeys, LayerKeys, Linear, PackingKey
 from .params import CONFIG1, ParamSet
 
 
@@ -36,8 +36,8 @@ class SpikeModelConfig:
     log2_beta_x: int = 22
     gal_log2_beta: int = 4
     gal_l: int = 6
-    pk_log2_beta: int = 8
-    pk_l: int = 3
+    pk_log2_beta: int = 7          # digits in int8: the packing runs on the tensor cores
+    pk_l: int = 4
     sigma_rlwe: float = 1.0
     pbs: ParamSet = field(default_factory=lambda: CONFIG1)
 
@@ -147,7 +147,8 @@ def to_device(model: SpikeModel, device=None) -> DeviceModel:
     pbs = Keys.create(cfg.pbs, k.bsk, k.ksk_a, k.ksk_b)
     gk = GaloisKeys(model.galois, cfg.gal_log2_beta, cfg.gal_l, dev)
     ksp = torch.from_numpy(np.ascontiguousarray(model.ksp).view(np.int32)).to(dev)
-    lk = LayerKeys(pbs, gk, ksp, cfg.pk_log2_beta, cfg.pk_l)
+    lk = LayerKeys(pbs, gk, ksp, cfg.pk_log2_beta, cfg.pk_l,
+                   PackingKey(model.ksp, cfg.pk_log2_beta, cfg.pk_l, dev))
     per = cfg.hidden // cfg.n_lut
     layers = []
     for L in model.layers:

@@ -275,6 +275,21 @@ int tfhe_pack_lwes(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_b
                    const uint32_t* lwe_a, const uint32_t* lwe_b, int32_t T, int64_t S,
                    uint32_t* out, void* stream);
 
+/* Device-resident packing key for repeated packings: a copy of ksp
+ * (n_dim, l, 2, N) and, where the digits fit 8 bits (log2_beta <= 7) and the
+ * int32 sums cannot overflow, its int8 limbs for the tcgen05 tensor cores. */
+typedef struct tfhe_packing_key tfhe_packing_key;
+int tfhe_packing_key_create(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
+                            void* stream, tfhe_packing_key** out);
+int tfhe_packing_key_destroy(tfhe_packing_key* key);
+/* 1 when the key carries tensor-core limbs, else 0. */
+int tfhe_packing_key_uses_tensor_cores(const tfhe_packing_key* key);
+/* tfhe_pack_lwes with a packing key (packing, schemas/text_jax.py:211-239):
+ * on the tensor cores when the key has limbs, tensor_cores != 0 and lwe_a is
+ * 16-byte aligned, else on CUDA cores; same result either way. */
+int tfhe_pack_lwes_with_key(const tfhe_packing_key* key, const uint32_t* lwe_a, const uint32_t* lwe_b,
+                            int32_t T, int64_t S, uint32_t* out, int32_t tensor_cores, void* stream);
+
 /* out[s] = X^rot * x[s] + y[s] for RLWEs (S, 2, N); y may be NULL
  * (rotate_ciphertext, schemas/text_jax.py:348-362, and
  * sum_ciphertext_ciphertext, :24-41).  out may alias y, and x only if

@@ -196,3 +196,68 @@ def test_cipher_mlp_head_matches_oracle():
         wa, wb = LO.cipher_mlp(m["keys"], p, head, (cen(xs[0, s, 0]), cen(xs[0, s, 1])))
         assert np.array_equal(h64(got_a[s]), u(wa))
         assert np.array_equal(h64(got_b[s]), u(wb))
+
+
+@pytest.mark.parametrize("T", [1, 10, 256])
+def test_packing_key_tensor_cores_match_oracle(T):
+    """Packing on the tcgen05 tensor cores (base 2^7, 4 levels: int8 digits)
+    equals the CUDA-core packing and the oracle."""
+    from tfhe_b200 import client
+    from tfhe_b200.lstm import PackingKey
+    m = layer_material()
+    rng = np.random.default_rng(40 + T)
+    N, S = 256, 2
+    ksp = client.packing_key(m["sk"], m["sk"], 7, 4, 1.0, rng)
+    key = PackingKey(ksp, 7, 4, DEV)
+    assert key.tensor_cores
+    a = rnd(rng, (S, T, N))
+    b = rnd(rng, (S, T))
+    got_tc = key.pack(d32(a), d32(b), tensor_cores=1)
+    got_cc = key.pack(d32(a), d32(b), tensor_cores=0)
+    assert torch.equal(got_tc, got_cc)
+    for s in range(S):
+        pa, pb = LO.packing(a[s], b[s], cen(ksp[:, :, 0]), cen(ksp[:, :, 1]), 7, 4, N)
+        assert np.array_equal(h64(got_tc[s, 0]), u(pa))
+        assert np.array_equal(h64(got_tc[s, 1]), u(pb))
+    key.close()
+
+
+def test_packing_key_with_wide_digits_stays_on_cuda_cores():
+    from tfhe_b200.lstm import PackingKey
+    m = layer_material()
+    key = PackingKey(m["ksp"], PK_LOG2_BETA, PK_L, DEV)       # base 2^8: digits reach 128
+    assert not key.tensor_cores
+    rng = np.random.default_rng(50)
+    a = rnd(rng, (1, 5, 256))
+    b = rnd(rng, (1, 5))
+    got = key.pack(d32(a), d32(b))
+    pa, pb = LO.packing(a[0], b[0], m["layer"]["ksp_a"], m["layer"]["ksp_b"], PK_LOG2_BETA, PK_L, 256)
+    assert np.array_equal(h64(got[0, 0]), u(pa)) and np.array_equal(h64(got[0, 1]), u(pb))
+    key.close()
+
+
+def test_timestep_with_tensor_core_packing_matches_oracle():
+    from tfhe_b200 import client
+    from tfhe_b200.lstm import CipherSpikeLSTM, LayerKeys, PackingKey
+    m, keys, layer = device_layer()
+    rng = np.random.default_rng(60)
+    ksp = client.packing_key(m["sk"], m["sk"], 7, 4, 1.0, rng)
+    lk = LayerKeys(keys.pbs, keys.galois, torch.from_numpy(ksp.view(np.int32)).to(DEV), 7, 4,
+                   PackingKey(ksp, 7, 4, DEV))
+    L = m["layer"]
+    tc_layer = CipherSpikeLSTM(lk, INPUT_DIM, HIDDEN, N_LUT, layer.W_f, layer.W_i, layer.W_o,
+                               L["lut_f"], L["lut_i"], L["lut_o"])
+    oracle_layer = dict(L, ksp_a=cen(ksp[:, :, 0]), ksp_b=cen(ksp[:, :, 1]), pk_log2_beta=7, pk_l=4)
+    N = m["p"]["N"]
+    xs, _ = encrypt_inputs(m["sk"], 2, 2, N, seed=61)
+    H = torch.zeros((2, 2, N), dtype=torch.int32, device=DEV)
+    C = torch.zeros_like(H)
+    oh = [(np.zeros(N, np.int64), np.zeros(N, np.int64)) for _ in range(2)]
+    oc = [(np.zeros(N, np.int64), np.zeros(N, np.int64)) for _ in range(2)]
+    for t in range(2):
+        H, C = tc_layer.step(d32(xs[t]), H, C)
+        for s in range(2):
+            oh[s], oc[s] = LO.spike_lstm_step(m["keys"], m["p"], oracle_layer, (cen(xs[t, s, 0]), cen(xs[t, s, 1])),
+                                              oh[s], oc[s])
+            assert np.array_equal(h64(H[s, 0]), u(oh[s][0])) and np.array_equal(h64(H[s, 1]), u(oh[s][1]))
+            assert np.array_equal(h64(C[s, 0]), u(oc[s][0])) and np.array_equal(h64(C[s, 1]), u(oc[s][1]))
