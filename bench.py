@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample", type=int, default=96, help="ciphertexts in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-per-core", type=int, default=8,
+                    help="ciphertexts per host core in each step of the reference arm")
     ap.add_argument("--lstm", action="store_true",
                     help="one encrypted Spike-LSTM layer + head: sequences/s (one GPU)")
     ap.add_argument("--seq-len", type=int, default=32)
@@ -613,19 +615,21 @@ def _set_single_thread():
 def run_reference(args, rank, world):
     """The reference arm: the CPU statement of the path timed on the host
     cores with all threads (one process per core), on the engine arm's
-    workload; each step is a bounded sample of one ciphertext per core."""
+    workload; each step is a bounded sample of --ref-per-core ciphertexts per
+    core (one batch per process, as the reference's batched path would)."""
     if rank != 0:
         return None
     import numpy as np
     from tfhe_b200.params import CONFIG2
     cores = os.cpu_count() or 1
+    per = max(1, args.ref_per_core)
     steps = args.warmup + args.steps
-    keys, msgs, a, b, lut, expect = make_inputs(CONFIG2, cores * steps, args.seed)
+    keys, msgs, a, b, lut, expect = make_inputs(CONFIG2, cores * per * steps, args.seed)
     st = CpuStatement(args.seed, cores)
     walls, errors = [], 0
     try:
         for s in range(steps):
-            sl = slice(s * cores, (s + 1) * cores)
+            sl = slice(s * cores * per, (s + 1) * cores * per)
             wall, dec = st.run(a[sl], b[sl], lut[sl])
             if s >= args.warmup:
                 walls.append(wall)
@@ -633,8 +637,8 @@ def run_reference(args, rank, world):
     finally:
         st.close()
     wall = sum(walls)
-    value = cores * args.steps / wall
-    sample = f"{cores} ciphertexts per step (one per process) of the batch-{args.batch} workload"
+    value = cores * per * args.steps / wall
+    sample = f"{cores * per} ciphertexts per step ({per} per process, {cores} processes) of the batch-{args.batch} workload"
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 1),
