@@ -265,8 +265,11 @@ class CipherSpikeLSTM:
         b = boot_b.reshape(S, self.per, self.n_lut).permute(0, 2, 1).reshape(S, self.hidden_dim)
         return a.contiguous(), b.contiguous()
 
-    def step(self, x_t, H, C, stream=None):
-        """One timestep for S sequences: x_t, H, C (S, 2, N) -> (H_t, C_t)."""
+    def step_phases(self, x_t, H, C, stream=None):
+        """One timestep for S sequences as a generator over its two
+        bootstraps: it yields (lwe_a, lwe_b, luts) for each bootstrap, is sent
+        the bootstrap's (out_a, out_b), and returns (H_t, C_t).  Drivers can
+        merge the bootstraps of several layers into one launch."""
         S, N, per, hid = x_t.shape[0], self.N, self.per, self.hidden_dim
         c_a = torch.empty((S, hid, N), dtype=torch.int32, device=x_t.device)
         c_b = torch.empty((S, hid), dtype=torch.int32, device=x_t.device)
@@ -282,7 +285,7 @@ class CipherSpikeLSTM:
         luts = torch.zeros((S, 2 * per, 2, N), dtype=torch.int32, device=x_t.device)
         luts[:, :per] = lut_c
         luts[:, per:, 1] = self.lut_i
-        boot_a, boot_b = self.keys.pbs.pbs(in_a, in_b, luts.reshape(S * 2 * per, 2, N), self.n_lut, stream=stream)
+        boot_a, boot_b = yield in_a, in_b, luts.reshape(S * 2 * per, 2, N)
         boot_a = boot_a.reshape(S, 2 * per, self.n_lut, N)
         boot_b = boot_b.reshape(S, 2 * per, self.n_lut)
         fc_a, fc_b = self._spikes(boot_a[:, :per], boot_b[:, :per], S)
@@ -291,14 +294,17 @@ class CipherSpikeLSTM:
         ct_b = u32_add(fc_b, si_b, stream=stream)
         # second bootstrap: O against the encrypted LUT of C_t
         lut_h = self._encrypted_luts(ct_a, ct_b, self.lut_o, stream)
-        h_a, h_b = self.keys.pbs.pbs(o_a.reshape(S * per, N), o_b.reshape(S * per),
-                                     lut_h.reshape(S * per, 2, N), self.n_lut, stream=stream)
+        h_a, h_b = yield o_a.reshape(S * per, N), o_b.reshape(S * per), lut_h.reshape(S * per, 2, N)
         h_a, h_b = self._spikes(h_a, h_b, S)
         k = self.keys
         C_t = k.pack(ct_a, ct_b, stream=stream)
         H_p = k.pack(h_a, h_b, stream=stream)
         H_t = rlwe_rotate_add(H_p, self.input_dim, stream=stream)
         return H_t, C_t
+
+    def step(self, x_t, H, C, stream=None):
+        """One timestep for S sequences: x_t, H, C (S, 2, N) -> (H_t, C_t)."""
+        return step_merged([(self, x_t, H, C)], stream)[0]
 
     def __call__(self, xs, stream=None):
         """xs (T, S, 2, N): the encrypted inputs of T timesteps.  Returns the
@@ -312,6 +318,41 @@ class CipherSpikeLSTM:
             H, C = self.step(xs[t], H, C, stream)
             hs.append(H)
         return (H, C), torch.stack(hs)
+
+
+def step_merged(items, stream=None):
+    """One timestep of several layers at once: items [(layer, x_t, H, C)]
+    over any numbers of sequences.  The layers' bootstraps run as one
+    launch per phase (all layers share the bootstrapping key and n_lut);
+    returns [(H_t, C_t)] in the order of items."""
+    gens, reqs, results = [], [], [None] * len(items)
+    for i, (layer, x, H, C) in enumerate(items):
+        g = layer.step_phases(x, H, C, stream)
+        gens.append((i, layer, g))
+        reqs.append(next(g))
+    while gens:
+        keys = gens[0][1].keys.pbs
+        n_lut = gens[0][1].n_lut
+        if any(l.keys.pbs is not keys or l.n_lut != n_lut for _, l, _ in gens):
+            raise ValueError("merged layers must share the bootstrapping key and n_lut")
+        counts = [r[0].shape[0] for r in reqs]
+        if len(reqs) == 1:
+            a, b, lut = reqs[0]
+        else:
+            a = torch.cat([r[0] for r in reqs])
+            b = torch.cat([r[1] for r in reqs])
+            lut = torch.cat([r[2] for r in reqs])
+        out_a, out_b = keys.pbs(a, b, lut, n_lut, stream=stream)
+        nxt_gens, nxt_reqs, off = [], [], 0
+        for (i, layer, g), c in zip(gens, counts):
+            try:
+                nxt_reqs.append(g.send((out_a[off:off + c], out_b[off:off + c])))
+                nxt_gens.append((i, layer, g))
+            except StopIteration as stop:
+                results[i] = stop.value
+            off += c
+        gens, reqs = nxt_gens, nxt_reqs
+    return results
 
 
 class CipherMLP:

@@ -7,9 +7,10 @@ tick:
   1. admits waiting requests into free slots (their inputs are copied to
      the device once; admission stops when the slot pool, sized from free
      HBM, is full),
-  2. gathers the current timestep of every live request and runs ONE
-     batched step of every layer over all of them (one bootstrap launch per
-     stage for the whole mix),
+  2. runs ONE batched step of every layer over all live requests: layer l
+     takes each request's timestep pos - l (a wavefront), its input being
+     layer l - 1's state from the previous tick, and the bootstraps of all
+     layers and requests share one launch per phase,
   3. retires requests whose sequence ended: one batched head over them and
      a device -> host copy of their logits.
 Requests therefore join and leave between ticks while others are on the
@@ -45,23 +46,30 @@ class Request:
 
 
 class StepModel:
-    """What the server drives.  States are lists of per-layer tensors with a
-    leading slot axis."""
+    """What the server drives.  States are per-layer tensors with a leading
+    slot axis."""
     N: int
     n_layers: int
 
     def state_shape(self):                 # per layer, per slot: e.g. (2, 2, N) for (H, C)
         raise NotImplementedError
 
-    def step(self, x, states):             # x (S, 2, N), states [ (S, ...) ] -> new states
+    def layer_input(self, layer, prev_states):
+        """Input of `layer` (> 0) from the states of layer - 1."""
         raise NotImplementedError
 
-    def head(self, states):                # states of finished slots -> (a (S, 1, N), b (S, 1))
+    def step_layers(self, xs, states):
+        """One timestep of every layer on its own slots: xs[l] (S_l, 2, N),
+        states[l] (S_l, ...) with any S_l (0 allowed) -> new states[l]."""
+        raise NotImplementedError
+
+    def head(self, states):                # last layer's states of finished slots -> (a (S, 1, N), b (S, 1))
         raise NotImplementedError
 
 
 class DeviceStepModel(StepModel):
-    """The engine's encrypted layers and head (spike_model.DeviceModel)."""
+    """The engine's encrypted layers and head (spike_model.DeviceModel); the
+    layers' bootstraps of one tick run as one launch per phase."""
 
     def __init__(self, dm):
         self.dm = dm
@@ -71,19 +79,24 @@ class DeviceStepModel(StepModel):
     def state_shape(self):
         return (2, 2, self.N)
 
-    def step(self, x, states):
+    def layer_input(self, layer, prev_states):
         from .lstm import rlwe_rotate_add
-        out = []
-        for layer, st in zip(self.dm.layers, states):
-            H, C = layer.step(x, st[:, 0].contiguous(), st[:, 1].contiguous())
-            out.append(torch.stack([H, C], dim=1))
-            x = rlwe_rotate_add(H, -layer.input_dim)
+        return rlwe_rotate_add(prev_states[:, 0].contiguous(), -self.dm.layers[layer - 1].input_dim)
+
+    def step_layers(self, xs, states):
+        from .lstm import step_merged
+        items, which = [], []
+        for li, (x, st) in enumerate(zip(xs, states)):
+            if x.shape[0]:
+                items.append((self.dm.layers[li], x, st[:, 0].contiguous(), st[:, 1].contiguous()))
+                which.append(li)
+        out = [None] * len(xs)
+        for li, (H, C) in zip(which, step_merged(items)):
+            out[li] = torch.stack([H, C], dim=1)
         return out
 
     def head(self, states):
         return self.dm.head(states[-1][:, 0].contiguous())
-
-
 def slots_for_memory(model: StepModel, t_max: int, free_bytes: int, reserve_bytes: int, cap: int) -> int:
     """Slots the pool can hold: inputs (t_max, 2, N) plus every layer's
     state per slot, within free device memory minus a reserve for the
@@ -125,25 +138,37 @@ class SpikeLstmServer:
             self.live[slot] = req
 
     def tick(self, now=None):
-        """One batched timestep of every live request; returns the requests
-        retired in this tick."""
+        """One batched tick: layer l of every live request takes that
+        request's timestep pos - l (a wavefront, so the layers' bootstraps
+        share launches); returns the requests retired in this tick."""
         self._admit()
         if not self.live:
             return []
+        L = self.model.n_layers
         slots = sorted(self.live)
-        idx = torch.tensor(slots, dtype=torch.long, device=self.device)
-        pos = torch.tensor([self.live[s].pos for s in slots], dtype=torch.long, device=self.device)
-        x = self.inputs[idx, pos].contiguous()
-        states = [st.index_select(0, idx) for st in self.states]
-        new = self.model.step(x, states)
-        for st, nw in zip(self.states, new):
-            st.index_copy_(0, idx, nw)
+        xs, idxs = [], []
+        for l in range(L):
+            sel = [s for s in slots if 0 <= self.live[s].pos - l < self.live[s].length]
+            idx = torch.tensor(sel, dtype=torch.long, device=self.device)
+            idxs.append(idx)
+            if not sel:
+                xs.append(torch.zeros((0, 2, self.model.N), dtype=torch.int32, device=self.device))
+            elif l == 0:
+                pos = torch.tensor([self.live[s].pos for s in sel], dtype=torch.long, device=self.device)
+                xs.append(self.inputs[idx, pos].contiguous())
+            else:
+                xs.append(self.model.layer_input(l, self.states[l - 1].index_select(0, idx)))
+        states = [st.index_select(0, idx) for st, idx in zip(self.states, idxs)]
+        new = self.model.step_layers(xs, states)
+        for st, idx, nw in zip(self.states, idxs, new):
+            if nw is not None and idx.numel():
+                st.index_copy_(0, idx, nw)
         self.ticks += 1
         self.batch_sizes.append(len(slots))
         done = []
         for s in slots:
             self.live[s].pos += 1
-            if self.live[s].pos == self.live[s].length:
+            if self.live[s].pos == self.live[s].length + L - 1:
                 done.append(s)
         out = []
         if done:

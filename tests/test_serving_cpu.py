@@ -19,14 +19,16 @@ class SumModel(StepModel):
     def state_shape(self):
         return (2, 2, self.N)
 
-    def step(self, x, states):
-        self.steps_seen.append(x.shape[0])
+    def layer_input(self, layer, prev_states):
+        return prev_states[:, 0]
+
+    def step_layers(self, xs, states):
+        self.steps_seen.append(max(x.shape[0] for x in xs))
         out = []
-        for st in states:
+        for x, st in zip(xs, states):
             H = st[:, 0] + x
             C = st[:, 1] + 1
             out.append(torch.stack([H, C], dim=1))
-            x = H
         return out
 
     def head(self, states):
@@ -63,8 +65,7 @@ def test_every_request_gets_its_own_result_in_any_mix():
         want_h, want_c = expected(r)
         assert torch.equal(r.logits[0][0], want_h)
         assert int(r.logits[1][0]) == want_c
-    assert max(model.steps_seen) == 3                       # never more live requests than slots
-    assert sum(model.steps_seen) == sum(r.length for r in reqs)
+    assert max(model.steps_seen) <= 3                       # never more live requests than slots
 
 
 def test_slots_are_reused_and_admission_waits():
@@ -75,7 +76,7 @@ def test_slots_are_reused_and_admission_waits():
         srv.submit(r)
     srv.tick()
     assert len(srv.live) == 2 and len(srv.waiting) == 1
-    srv.tick()                                               # a retires after its 2nd step
+    srv.tick()                                               # a (1 layer) retires after its 2nd step
     assert a.done is not None and a.slot is None
     srv.tick()                                               # c admitted into a's slot
     assert c.slot == 0 and len(srv.live) == 2
@@ -110,3 +111,16 @@ def test_real_time_arrivals_and_latency():
     assert s["count"] == 6 and 0 <= s["p50_s"] <= s["p99_s"]
     for r in reqs:
         assert torch.equal(r.logits[0][0], expected(r, 1)[0])
+
+
+def test_wavefront_takes_length_plus_depth_minus_one_ticks():
+    model = SumModel(layers=3)
+    srv = SpikeLstmServer(model, max_slots=2, t_max=8, device=torch.device("cpu"))
+    r = req(0, 5)
+    srv.submit(r)
+    ticks = 0
+    while not srv.idle():
+        srv.tick()
+        ticks += 1
+    assert ticks == 5 + 3 - 1
+    assert torch.equal(r.logits[0][0], expected(r, 3)[0])
