@@ -235,7 +235,15 @@ static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0) {
     BrShape s;
     int K = std::max(1, 512 / (2 * Q8));
     const int kreq = k_request > 0 ? k_request : k_override();
-    if (kreq > 0) K = std::min(K, kreq);
+    if (kreq > 0) {
+        K = std::min(K, kreq);
+    } else {
+        // a batch smaller than one full wave: spread it over every SM, since
+        // a CTA's time grows with its ciphertext count while idle SMs add nothing
+        const long long sms = std::max(1, sm_count());
+        const long long per_sm = (B + sms - 1) / sms;
+        if (per_sm < K) K = (int)std::max<long long>(1, per_sm);
+    }
     K = (int)std::min<long long>(K, std::max<long long>(B, 1));
     const int KT = (K % 2 == 0 && br_kt(ilog2(N), L) == 2) ? 2 : 1;
     while (K >= KT) {
