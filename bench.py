@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--seqs", type=int, default=16)
     ap.add_argument("--hidden", type=int, default=128)
     ap.add_argument("--layers", type=int, default=1)
+    ap.add_argument("--graph", action="store_true", help="--lstm: replay each timestep from a CUDA graph")
     ap.add_argument("--serve", action="store_true",
                     help="continuous-batching server with Poisson arrivals: p50/p99 latency and sequences/s")
     ap.add_argument("--rate", type=float, default=2.0, help="requests per second (--serve)")
@@ -303,8 +304,18 @@ def run_lstm(args):
     xs_d = xs_h.to(dev)
     stream = torch.cuda.current_stream()
 
+    graphs = None
+    if args.graph:
+        from tfhe_b200.lstm import StepGraph
+        if cfg.layers != 1:
+            raise SystemExit("--graph supports one layer")
+        graphs = StepGraph(dm.layers[0], args.seqs)
+
     def forward(xs):
-        H, _ = SM.run_layers(dm, xs)
+        if graphs is not None:
+            H, _ = graphs.run(xs)
+        else:
+            H, _ = SM.run_layers(dm, xs)
         return dm.head(H)
 
     for _ in range(args.warmup):
@@ -343,6 +354,7 @@ def run_lstm(args):
             "ms_per_step": round(dev_ms, 2), "higher_is_better": True, "dtype": "u32 torus, f64 FFT",
             "data": "synthetic: Zipf(1.1) tokens over 8192, random int weights / embeddings / thresholds",
             "config": {"workload": "Spike-LSTM", "seqs": args.seqs, "seq_len": args.seq_len, "emb_dim": cfg.emb_dim,
+                       "timestep": "CUDA graph" if args.graph else "direct launches",
                        "hidden": cfg.hidden, "layers": cfg.layers, "n_lut": cfg.n_lut, "pbs": cfg.pbs.name,
                        "weights": "[-7, 7]"},
             "e2e": {"value": round(args.seqs / e2e_ms * 1e3, 3), "unit": "seq/s",

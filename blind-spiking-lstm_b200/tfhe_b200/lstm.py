@@ -355,6 +355,45 @@ def step_merged(items, stream=None):
     return results
 
 
+class StepGraph:
+    """One CipherSpikeLSTM timestep for S sequences captured in a CUDA graph
+    on fixed device buffers (x, H, C -> H_out, C_out); run() replays it once
+    per timestep, so a sequence costs one graph launch per token instead of
+    the step's ~25 kernel launches and their host work."""
+
+    def __init__(self, layer: "CipherSpikeLSTM", S: int, stream=None):
+        dev = layer.device
+        N = layer.N
+        self.layer = layer
+        self.x = torch.zeros((S, 2, N), dtype=torch.int32, device=dev)
+        self.H = torch.zeros_like(self.x)
+        self.C = torch.zeros_like(self.x)
+        layer.step(self.x, self.H, self.C)        # uncaptured: kernel attributes, status word, allocator
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.H_out, self.C_out = layer.step(self.x, self.H, self.C)
+
+    def step(self, x_t, H, C):
+        """(S, 2, N) inputs -> graph-owned (H_t, C_t), valid until the next replay."""
+        self.x.copy_(x_t)
+        self.H.copy_(H)
+        self.C.copy_(C)
+        self.graph.replay()
+        return self.H_out, self.C_out
+
+    def run(self, xs):
+        """xs (T, S, 2, N) from zero state -> final (H, C) (copies)."""
+        self.H.zero_()
+        self.C.zero_()
+        for t in range(xs.shape[0]):
+            self.x.copy_(xs[t])
+            self.graph.replay()
+            self.H.copy_(self.H_out)
+            self.C.copy_(self.C_out)
+        return self.H.clone(), self.C.clone()
+
+
 class CipherMLP:
     """CipherMLP (nn_tfhe/Spike_LSTM.py:187-206) with the ReLU bootstrap of
     ReluBoostrapper (nn_tfhe/activation.py:166-237): linear1, one bootstrap

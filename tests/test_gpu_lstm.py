@@ -261,3 +261,19 @@ def test_timestep_with_tensor_core_packing_matches_oracle():
                                               oh[s], oc[s])
             assert np.array_equal(h64(H[s, 0]), u(oh[s][0])) and np.array_equal(h64(H[s, 1]), u(oh[s][1]))
             assert np.array_equal(h64(C[s, 0]), u(oc[s][0])) and np.array_equal(h64(C[s, 1]), u(oc[s][1]))
+
+
+def test_timestep_graph_replay_equals_direct_steps():
+    """The CUDA-graph timestep (StepGraph) reproduces direct steps bit for bit."""
+    from tfhe_b200.lstm import StepGraph
+    m, keys, layer = device_layer()
+    N = m["p"]["N"]
+    xs, _ = encrypt_inputs(m["sk"], 3, 2, N, seed=71)
+    xs_d = d32(xs)
+    g = StepGraph(layer, 2)
+    Hg, Cg = g.run(xs_d)
+    H = torch.zeros((2, 2, N), dtype=torch.int32, device=DEV)
+    C = torch.zeros_like(H)
+    for t in range(3):
+        H, C = layer.step(xs_d[t], H, C)
+    assert torch.equal(Hg, H) and torch.equal(Cg, C)
