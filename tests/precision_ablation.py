@@ -100,9 +100,10 @@ def torus(x64):
 class Study:
     """One sample of ciphertexts with every form's chain."""
 
-    def __init__(self, samples, seed=0, groups=None):
-        name = "cfg1"
+    def __init__(self, samples, seed=0, groups=None, name="cfg1", n_lut=N_LUT, t_in=T_IN, t_out=T_OUT,
+                 fp32=True):
         p = PARAMS[name]
+        self.n_lut, self.t_in, self.t_out = n_lut, t_in, t_out
         self.p = p
         self.k = case_keys(name)
         N, n, c = p["N"], p["n"], p["collapse"]
@@ -110,15 +111,15 @@ class Study:
         self.G = n // c if groups is None else groups
         self.M = 2 ** c
         rng = np.random.default_rng(1000 + seed)
-        self.msgs = rng.integers(0, T_IN // 2, size=samples)
-        a, b = O.encrypt_inputs(self.k, self.msgs, Q / T_IN, rng)
+        self.msgs = rng.integers(0, t_in // 2, size=samples)
+        a, b = O.encrypt_inputs(self.k, self.msgs, Q / t_in, rng)
         a, b = canon(a), canon(b)
         ka, kb = O.key_switch_LWE(self.k.ksk, (a, b), ks_params(name))
         self.ka, self.kb = ka, np.asarray(kb).reshape(-1)
-        self.idx = O.rotation_indices(self.ka, c, N, Q, N_LUT)                 # (B, G, M)
-        self.tables = rng.integers(0, T_OUT // 2, size=(N_LUT, T_IN // 2))
+        self.idx = O.rotation_indices(self.ka, c, N, Q, n_lut)                 # (B, G, M)
+        self.tables = rng.integers(0, t_out // 2, size=(n_lut, t_in // 2))
         self.expect = self.tables[:, self.msgs].T                              # (B, n_lut)
-        body = client.packed_table_lut(N, self.tables, T_OUT)
+        body = client.packed_table_lut(N, self.tables, t_out)
         self.acc0 = np.zeros((samples, 2, N))
         self.acc0[:, 1] = canon(body.view(np.int32).astype(np.float64))
         # keys in every form
@@ -127,7 +128,7 @@ class Study:
                             for t, lb in enumerate(O._limbs(key)) if np.any(lb)]
         self.fp64_key = O.bsk_reshape(self.k.bsk_ordered, n // c, c)
         self.fp32_keys = {cnt: [(O.jax_fourier(lb.astype(np.float64)).astype(np.complex64), s)
-                                for lb, s in split_limbs(key, cnt)] for cnt in (2, 3, 4)}
+                                for lb, s in split_limbs(key, cnt)] for cnt in (2, 3, 4)} if fp32 else {}
         self.ang64 = np.exp(-1j * np.pi * np.outer(np.arange(2 * N), 2 * np.arange(N // 2) + 1) / N)
         self.ang32 = self.ang64.astype(np.complex64)
         self.rot64 = O.all_rot_possible_fourier(N)
@@ -194,18 +195,18 @@ class Study:
                     st[1] += float(np.sum(e * e))
                     st[2] += e.size
                 accs[f] = mine.astype(np.float64)
-        b_rot = O.body_rotation(self.kb, self.N, Q, N_LUT)
+        b_rot = O.body_rotation(self.kb, self.N, Q, self.n_lut)
         for f in ("exact",) + tuple(forms):
             alphas = np.repeat(-b_rot.astype(np.int64)[:, None], 2, axis=1)
             rotated = O.coef_rotation_rows(accs[f], alphas)
-            a_out, b_out = O.extract_many(rotated, N_LUT)
+            a_out, b_out = O.extract_many(rotated, self.n_lut)
             a_out = np.asarray(a_out).reshape(-1, self.N)
             b_out = np.asarray(b_out).reshape(-1)
             phase = torus(np.rint(b_out).astype(np.int64) -
                           np.rint(a_out @ self.k.sk_glwe).astype(np.int64))
-            want = self.expect.reshape(-1) * (2 ** 32 // T_OUT)
+            want = self.expect.reshape(-1) * (2 ** 32 // self.t_out)
             noise = torus(phase - want).astype(np.float64)
-            dec = np.mod(np.rint(phase / (2.0 ** 32 / T_OUT)), T_OUT).astype(np.int64)
+            dec = np.mod(np.rint(phase / (2.0 ** 32 / self.t_out)), self.t_out).astype(np.int64)
             fails = int(np.sum(dec != self.expect.reshape(-1)))
             entry = {"output_noise_std": float(np.std(noise)), "output_noise_max": float(np.max(np.abs(noise))),
                      "failures": fails, "outputs": int(noise.size)}
@@ -215,9 +216,9 @@ class Study:
                 entry.update({"group_err_max": mx, "group_err_var": s2 / max(cnt, 1),
                               "final_diff_max": float(np.max(np.abs(d))), "final_diff_var": float(np.mean(d * d))})
             sigma = entry["output_noise_std"]
-            thr = 2.0 ** 32 / (2 * T_OUT)
+            thr = 2.0 ** 32 / (2 * self.t_out)
             p_fail = math.erfc(thr / (sigma * math.sqrt(2))) if sigma > 0 else 0.0
-            entry["expected_failures_per_1e6_pbs"] = p_fail * 1e6 * N_LUT
+            entry["expected_failures_per_1e6_pbs"] = p_fail * 1e6 * self.n_lut
             res[f] = entry
         return res
 
@@ -233,15 +234,22 @@ def main():
     ap.add_argument("--samples", type=int, default=16)
     ap.add_argument("--groups", type=int, default=None)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--params", choices=["cfg1", "cfg2"], default="cfg1",
+                    help="cfg1: 4 LUTs, Z_4, every form; cfg2 (gadget 2^15 x 2): 1 LUT, Z_8 inputs, FP64 only")
     args = ap.parse_args()
     t0 = time.time()
-    st = Study(args.samples, args.seed, args.groups)
-    res = st.run()
-    print(f"# {args.samples} PBS x {N_LUT} outputs, {st.G} groups, {time.time() - t0:.0f} s")
+    if args.params == "cfg1":
+        st = Study(args.samples, args.seed, args.groups)
+        forms = FORMS
+    else:
+        st = Study(args.samples, args.seed, args.groups, name="cfg2", n_lut=1, t_in=16, t_out=8, fp32=False)
+        forms = ("fp64",)
+    res = st.run(forms)
+    print(f"# {args.params}: {args.samples} PBS x {st.n_lut} outputs, {st.G} groups, {time.time() - t0:.0f} s")
     print("| form | per-group error max | per-group error var | final phase diff max | final phase diff var | "
           "output noise std | failures (sample) | expected failures / 10^6 PBS |")
     print("|---|---:|---:|---:|---:|---:|---:|---:|")
-    for f in ("exact",) + FORMS:
+    for f in ("exact",) + tuple(forms):
         e = res[f]
         print(f"| {f} | {_fmt(e.get('group_err_max', 0))} | {_fmt(e.get('group_err_var', 0))} | "
               f"{_fmt(e.get('final_diff_max', 0))} | {_fmt(e.get('final_diff_var', 0))} | "
