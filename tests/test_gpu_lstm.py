@@ -277,3 +277,24 @@ def test_timestep_graph_replay_equals_direct_steps():
     for t in range(3):
         H, C = layer.step(xs_d[t], H, C)
     assert torch.equal(Hg, H) and torch.equal(Cg, C)
+
+
+def test_packing_key_unaligned_input_uses_cuda_cores():
+    """LWE masks that are not 16-byte aligned take the CUDA-core packing (the
+    tensor-core kernel loads 16-byte vectors) with the same result."""
+    from tfhe_b200 import client
+    from tfhe_b200.lstm import PackingKey
+    m = layer_material()
+    rng = np.random.default_rng(80)
+    ksp = client.packing_key(m["sk"], m["sk"], 7, 4, 1.0, rng)
+    key = PackingKey(ksp, 7, 4, DEV)
+    a = rnd(rng, (1, 6, 256))
+    b = rnd(rng, (1, 6))
+    big = torch.zeros((a.size + 1,), dtype=torch.int32, device=DEV)
+    big[1:] = d32(a).reshape(-1)
+    a_view = big[1:].view(1, 6, 256)
+    assert a_view.data_ptr() % 16 != 0
+    got = key.pack(a_view, d32(b))
+    pa, pb = LO.packing(a[0], b[0], cen(ksp[:, :, 0]), cen(ksp[:, :, 1]), 7, 4, 256)
+    assert np.array_equal(h64(got[0, 0]), u(pa)) and np.array_equal(h64(got[0, 1]), u(pb))
+    key.close()
