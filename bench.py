@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=16384)
+    ap.add_argument("--params", choices=["cfg2", "cfg1"], default="cfg2",
+                    help="engine arm and sweep: the 2048 set (default) or the 1024 set (n=630, gadget 2^7 x 3, c=3)")
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample", type=int, default=96, help="ciphertexts in the CPU baseline sample")
@@ -154,11 +156,11 @@ def run_engine(args, rank, world, local_rank, dist):
     import torch
     from tfhe_b200 import client
     from tfhe_b200.engine import Keys, probe_fp64_peak
-    from tfhe_b200.params import CONFIG2
+    from tfhe_b200.params import CONFIG1, CONFIG2
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    p = CONFIG2
+    p = CONFIG1 if args.params == "cfg1" else CONFIG2
     B = args.batch
     keys, msgs, a, b, lut, expect = make_inputs(p, B, args.seed + rank)
     eng = Keys.create(p, keys.bsk, keys.ksk_a, keys.ksk_b)
@@ -252,21 +254,22 @@ def run_engine(args, rank, world, local_rank, dist):
     e2e_value = total / (e2e_ms * 1e-3)
     fl = flops_per_pbs(p)
     achieved_tf = B * fl / (br_ms * 1e-3) / 1e12
-    traffic = read_traffic(B)
+    traffic = read_traffic(B) if args.params == "cfg2" else None   # the committed capture is of the 2048 set
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_name(p, B), "params": p.name, "batch_per_gpu": B, "n_lut": 1,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "inputs larger than L2: 402 MB of ciphertexts and LUTs per step, 195 MB key"},
+                   "l2": f"inputs larger than L2: {(a_h.numel() + b_h.numel() + lut_h.numel()) * 4 / 1e6:.0f} MB of "
+                         f"ciphertexts and LUTs per step, {p.bsk_bytes_fp64() / 1e6:.0f} MB key"},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
                 "h2d_bytes_per_step": int(a_h.numel() * 4 + b_h.numel() * 4 + lut_h.numel() * 4),
                 "d2h_bytes_per_step": int(oa_h.numel() * 4 + ob_h.numel() * 4),
                 "outputs_equal_device_arm": not bool(e2e_diff)},
         "roofline": {"bound": "fp64", "achieved": round(achieved_tf, 3), "peak": round(peak_fp64, 3),
                      "unit": "TFLOP/s", "frac": round(achieved_tf / peak_fp64, 4), "traffic": traffic,
-                     "kernel": "br_fp64_kernel<11,2> (blind rotation + extraction)",
+                     "kernel": f"br_fp64_kernel<{p.N.bit_length() - 1},{p.l_bs}> (blind rotation + extraction)",
                      "flops_per_pbs": int(fl), "launch_ms": round(br_ms, 3),
                      "peak_source": "FP64 FMA probe (tfhe_probe_fp64_fma) on this GPU; MEASURED_PEAKS.json "
                                     "holds no FP64 figure",
@@ -465,11 +468,11 @@ def run_sweep(args, batches):
     from tfhe_b200 import client
     from tfhe_b200.autotune import autotune
     from tfhe_b200.engine import Keys, PBSGraph
-    from tfhe_b200.params import CONFIG2
+    from tfhe_b200.params import CONFIG1, CONFIG2
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
-    p = CONFIG2
+    p = CONFIG1 if args.params == "cfg1" else CONFIG2
     bmax = max(batches)
     keys, msgs, a, b, lut, expect = make_inputs(p, bmax, args.seed)
     eng = Keys.create(p, keys.bsk, keys.ksk_a, keys.ksk_b)
@@ -521,7 +524,8 @@ def run_sweep(args, batches):
         same = bool(torch.equal(graph.out_a, oa) and torch.equal(graph.out_b, ob))
         del graph
         eng.set_tuning()
-        out.append({"sweep": "PBS+KS n=742 N=2048 gadget 2^15x2 KS 2^4x5 c=2", "batch": B, "steps": steps,
+        out.append({"sweep": f"PBS+KS n={p.n} N={p.N} gadget 2^{p.log2_beta_bs}x{p.l_bs} KS 2^{p.log2_beta_ks}x{p.l_ks} "
+                              f"c={p.collapse}", "batch": B, "steps": steps,
                     "plain": {"ms_per_batch": round(plain_ms, 4), "PBS/s": round(B / plain_ms * 1e3, 1),
                               "decrypt_errors": plain_err, "K": plain_shape[0], "persistent": 0},
                     "persistent_autotuned_graph": {"ms_per_batch": round(tuned_ms, 4),

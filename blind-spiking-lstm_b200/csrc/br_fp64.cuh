@@ -191,6 +191,20 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     __syncthreads();
 
     for (int g = 0; g < args.G; ++g) {
+        if constexpr (KR == 0 && !REFLAYOUT) {
+            // the next group's key block (all CTAs together: each its share)
+            // into L2 while this group runs
+            if (tid == 0 && g + 1 < args.G) {
+                const size_t block = (size_t)2 * P * M * H * sizeof(double2);
+                const size_t share = ((block / gridDim.x) + 255) & ~(size_t)255;
+                const size_t off = (size_t)blockIdx.x * share;
+                if (off < block) {
+                    const size_t len = min(share, block - off);
+                    const char* base = reinterpret_cast<const char*>(args.bsk + (size_t)(g + 1) * 2 * P * M * H);
+                    prefetch_l2_bulk(base + off, (uint32_t)len);
+                }
+            }
+        }
         // rotation index of every (ciphertext, pattern) of this group
         for (int t = tid; t < K * M; t += nt) {
             const int k = t / M;
