@@ -920,7 +920,16 @@ int tfhe_pbs_host(const tfhe_keys* keys, const uint32_t* a_host, const uint32_t*
     if (n_lut < 1 || n_lut > keys->p.N) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut out of range");
     cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
     const tfhe_params& p = keys->p;
-    long long C = chunk > 0 ? chunk : std::max<long long>(2048, ((batch + 7) / 8 + 2047) / 2048 * 2048);
+    // automatic chunks: about an eighth of the batch, a whole number of
+    // blind-rotation waves (SMs x ciphertexts per CTA) so no chunk ends on a
+    // partly idle wave
+    long long C = chunk;
+    if (C == 0) {
+        const BrShape sh = br_shape(p.N, p.l_bs, keys->M, std::max<long long>(batch, 1 << 20),
+                                    keys->tune.ciphertexts_per_cta);
+        const long long wave = (long long)std::max(1, sm_count()) * std::max(1, sh.K);
+        C = std::max<long long>(wave, ((batch + 7) / 8 + wave - 1) / wave * wave);
+    }
     C = std::min<long long>(C, batch);
     const size_t N = (size_t)p.N, nb = (size_t)p.n_big, n = (size_t)p.n;
     const bool lut_per_ct = lut_count == batch && batch > 1;
