@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--serve", action="store_true",
                     help="continuous-batching server with Poisson arrivals: p50/p99 latency and sequences/s")
     ap.add_argument("--rate", type=float, default=2.0, help="requests per second (--serve)")
-    ap.add_argument("--requests", type=int, default=24, help="requests per serving run (--serve)")
+    ap.add_argument("--requests", type=int, default=48, help="requests per serving run (--serve)")
     ap.add_argument("--max-slots", type=int, default=64)
     ap.add_argument("--sweep", default=None,
                     help="comma-separated batch sizes: print one line per batch comparing the plain launch with "

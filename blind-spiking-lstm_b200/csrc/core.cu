@@ -334,12 +334,13 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     args.K = sh.K;
     args.ring_stages = sh.stages;
     args.wait_limit = WAIT_LIMIT_CYCLES;
-    // L1 prefetch of the next pattern's key words: by default where a thread
-    // loads one output's key words at a time (measured +5% there, -4% where
-    // both outputs' words are already in flight); TFHE_B200_PREFETCH=0/1 forces
+    // L1 prefetch of the next pattern's key words: off by default.  With the
+    // next group's key block prefetched into L2 it costs time at every
+    // parameter set measured (n=630 N=1024: 181.2 ms off vs 207.8 ms on per
+    // 16384 ciphertexts); TFHE_B200_PREFETCH=1 or the keys' tuning turns it on
     static const int prefetch_env = [] {
         const char* env = getenv("TFHE_B200_PREFETCH");
-        return env ? (env[0] == '1' ? 1 : 0) : -1;
+        return env ? (env[0] == '1' ? 1 : 0) : 0;
     }();
     args.prefetch = (tune && tune->prefetch >= 0) ? tune->prefetch : prefetch_env;
     args.status = status ? status : device_status_word();

@@ -56,7 +56,7 @@ typedef struct tfhe_keys tfhe_keys;   /* device-resident key material */
  * the reference; chosen by an autotuner or left automatic). */
 typedef struct tfhe_tuning {
     int32_t ciphertexts_per_cta;  /* 0: as many as shared memory and 512 threads allow */
-    int32_t prefetch;             /* L1 prefetch of key words: -1 automatic, 0 off, 1 on */
+    int32_t prefetch;             /* L1 prefetch of key words: -1 automatic (off), 0 off, 1 on */
     int32_t persistent;           /* CTAs loop over ciphertext sets: -1 automatic (on), 0, 1 */
     int32_t ks_tensor_cores;      /* key switch on tcgen05 int8 tensor cores: -1 automatic (on
                                      where the parameters allow), 0 off (CUDA cores), 1 on */
