@@ -101,7 +101,9 @@ __device__ __forceinline__ void forward_middle(double2* dec, int npoly, const do
 // shared-memory ring by 1D bulk copies; the device key layout is then
 // [G][4/KR parts][2 out][M][P][NT slots] so each (group, part, out, pattern)
 // chunk of P * NT words is contiguous (NT = KR H / 4 = threads per CTA).
-template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP>
+// QTG: the quarter root table is read from global memory (L1-cached) instead
+// of shared memory, so two CTAs of half the ciphertexts fit on one SM.
+template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP, bool QTG = false>
 __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp64_kernel(const BrArgs args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
@@ -115,8 +117,9 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     const int K = args.K;
     const int M = args.M;
     double2* dec = reinterpret_cast<double2*>(smem_raw);           // K * P * H
-    double2* qt = dec + (size_t)K * P * H;                          // N / 2
-    double2* tw = qt + N / 2;                                       // PL::TW
+    double2* qt_s = dec + (size_t)K * P * H;                        // N / 2 (unless QTG)
+    const double2* qt = QTG ? args.qt : qt_s;
+    double2* tw = QTG ? qt_s : qt_s + N / 2;                        // PL::TW
     uint16_t* freq = reinterpret_cast<uint16_t*>(tw + PL::TW);      // H
     int* rot = reinterpret_cast<int*>(freq + H);                    // K * M
     int* bexp = rot + K * M;                                        // K
@@ -132,7 +135,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     const long long nsets = (args.B + K - 1) / K;
     const long long my_sets = blockIdx.x < nsets ? (nsets - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
-    for (int i = tid; i < N / 2; i += nt) qt[i] = args.qt[i];
+    if constexpr (!QTG)
+        for (int i = tid; i < N / 2; i += nt) qt_s[i] = args.qt[i];
     for (int i = tid; i < PL::TW; i += nt) tw[i] = args.tw[i];
     for (int i = tid; i < H; i += nt) freq[i] = args.freq[i];
 

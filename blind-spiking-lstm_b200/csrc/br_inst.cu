@@ -12,13 +12,15 @@
 
 namespace tfhe {
 
-BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt) {
+BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt, bool qtg) {
 #define TFHE_BR_CASE(LL)                                                                         \
     case LL:                                                                                     \
         if (reflayout) return kt == 2 ? br_fp64_kernel<BR_LOGN, LL, true, 0, 2>                    \
                                       : br_fp64_kernel<BR_LOGN, LL, true, 0, 1>;                   \
         if (kr == 2) return br_fp64_kernel<BR_LOGN, LL, false, 2, 1>;                             \
         if (kr != 0) return nullptr;                                                             \
+        if (qtg) return kt == 2 ? br_fp64_kernel<BR_LOGN, LL, false, 0, 2, true>                   \
+                                : br_fp64_kernel<BR_LOGN, LL, false, 0, 1, true>;                  \
         return kt == 2 ? br_fp64_kernel<BR_LOGN, LL, false, 0, 2> : br_fp64_kernel<BR_LOGN, LL, false, 0, 1>;
     switch (L) {
         TFHE_BR_CASE(1)

@@ -214,7 +214,16 @@ struct BrShape {
     size_t smem = 0;
     int kr = 0, stages = 0;   // key ring (kr > 0)
     int kt = 1;               // ciphertexts per thread in the pointwise stage
+    bool qtg = false;         // quarter root table in global memory (two CTAs per SM)
 };
+
+static int max_smem_per_sm() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    return v;
+}
+
 
 // a mbarrier wait gives up after this many cycles (about 2 s)
 
@@ -228,7 +237,7 @@ static int k_override() {
     return v;
 }
 
-static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0) {
+static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0, bool allow_qtg = false) {
     const int H = N / 2, Q8 = H / 8;
     const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
     const size_t limit = (size_t)max_smem_optin();
@@ -253,6 +262,22 @@ static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0) {
             s.nt = K * 2 * Q8;
             s.smem = smem;
             s.kt = (K % KT == 0) ? KT : 1;
+            // two CTAs per SM where they fit once the quarter root table is
+            // read from global memory (automatic shapes halve K for it): their
+            // phases drift apart, so one CTA's FFT overlaps the other's key
+            // loads (n=630 N=1024: 181.2 -> 166.8 ms per 16384 ciphertexts)
+            if (allow_qtg && s.kt == 2) {
+                const int K2 = (kreq <= 0 && K % 4 == 0) ? K / 2 : K;
+                const size_t smem2 = per_ct * K2 + br_table_bytes(N) - (size_t)(N / 2) * sizeof(double2) +
+                                     (size_t)(K2 * M + K2) * sizeof(int) + 16;
+                if (2 * (smem2 + 1024) <= (size_t)max_smem_per_sm()) {
+                    s.K = K2;
+                    s.nt = K2 * 2 * Q8;
+                    s.smem = smem2;
+                    s.kt = 2;
+                    s.qtg = true;
+                }
+            }
             return s;
         }
         K -= KT;
@@ -318,9 +343,9 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
                      int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
-                              : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0);
+                              : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0, !reflayout);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
-    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt);
+    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt, sh.qtg);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
     if (sh.K < 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT,
@@ -927,8 +952,8 @@ int tfhe_pbs_host(const tfhe_keys* keys, const uint32_t* a_host, const uint32_t*
     long long C = chunk;
     if (C == 0) {
         const BrShape sh = br_shape(p.N, p.l_bs, keys->M, std::max<long long>(batch, 1 << 20),
-                                    keys->tune.ciphertexts_per_cta);
-        const long long wave = (long long)std::max(1, sm_count()) * std::max(1, sh.K);
+                                    keys->tune.ciphertexts_per_cta, true);
+        const long long wave = (long long)std::max(1, sm_count()) * std::max(1, sh.K) * (sh.qtg ? 2 : 1);
         C = std::max<long long>(wave, ((batch + 7) / 8 + wave - 1) / wave * wave);
     }
     C = std::min<long long>(C, batch);
@@ -1049,7 +1074,7 @@ int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* cipher
     const tfhe_params& p = keys->p;
     const BrShape sh = keys->ring_kr > 0 ? ring_shape(p.N, p.l_bs, keys->M)
                                          : br_shape(p.N, p.l_bs, keys->M, std::max<int64_t>(batch, 1),
-                                                    keys->tune.ciphertexts_per_cta);
+                                                    keys->tune.ciphertexts_per_cta, true);
     *ciphertexts_per_cta = sh.K;
     *threads = sh.nt;
     *shared_bytes = (int64_t)sh.smem;

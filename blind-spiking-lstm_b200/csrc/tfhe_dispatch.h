@@ -10,7 +10,7 @@ using BrKernel = void (*)(const BrArgs);
 using BrConvKernel = void (*)(const BskConvArgs);
 
 #define TFHE_DECLARE_LOGN(LG)                              \
-    BrKernel br_fp64_logn_##LG(int L, bool reflayout, int kr, int kt);     \
+    BrKernel br_fp64_logn_##LG(int L, bool reflayout, int kr, int kt, bool qtg);     \
     BrConvKernel bsk_fft_logn_##LG();
 
 TFHE_DECLARE_LOGN(7)
@@ -21,14 +21,14 @@ TFHE_DECLARE_LOGN(11)
 TFHE_DECLARE_LOGN(12)
 #undef TFHE_DECLARE_LOGN
 
-inline BrKernel br_fp64_kernel_for(int logn, int L, bool reflayout, int kr, int kt) {
+inline BrKernel br_fp64_kernel_for(int logn, int L, bool reflayout, int kr, int kt, bool qtg = false) {
     switch (logn) {
-        case 7: return br_fp64_logn_7(L, reflayout, kr, kt);
-        case 8: return br_fp64_logn_8(L, reflayout, kr, kt);
-        case 9: return br_fp64_logn_9(L, reflayout, kr, kt);
-        case 10: return br_fp64_logn_10(L, reflayout, kr, kt);
-        case 11: return br_fp64_logn_11(L, reflayout, kr, kt);
-        case 12: return br_fp64_logn_12(L, reflayout, kr, kt);
+        case 7: return br_fp64_logn_7(L, reflayout, kr, kt, qtg);
+        case 8: return br_fp64_logn_8(L, reflayout, kr, kt, qtg);
+        case 9: return br_fp64_logn_9(L, reflayout, kr, kt, qtg);
+        case 10: return br_fp64_logn_10(L, reflayout, kr, kt, qtg);
+        case 11: return br_fp64_logn_11(L, reflayout, kr, kt, qtg);
+        case 12: return br_fp64_logn_12(L, reflayout, kr, kt, qtg);
         default: return nullptr;
     }
 }

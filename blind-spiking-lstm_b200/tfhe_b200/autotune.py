@@ -51,10 +51,11 @@ def save_cache(cache: dict, path: str = CACHE_PATH) -> None:
 
 
 def candidates(keys: Keys, batch: int):
-    """Shapes worth timing: automatic K and smaller K, prefetch auto/off/on,
+    """Shapes worth timing: the automatic shape (K = 0), the automatic K
+    requested explicitly and half of it, each with prefetch auto/off/on and
     persistent on/off."""
     kmax, _, _ = keys.launch_shape(batch)
-    ks = sorted({kmax, max(1, kmax // 2)}, reverse=True)
+    ks = [0] + sorted({kmax, max(1, kmax // 2)}, reverse=True)
     out = []
     for k in ks:
         for pf in (-1, 0, 1):
