@@ -274,7 +274,8 @@ def run_engine(args, rank, world, local_rank, dist):
                      "peak_source": "FP64 FMA probe (tfhe_probe_fp64_fma) on this GPU; MEASURED_PEAKS.json "
                                     "holds no FP64 figure",
                      "key_bytes_per_launch": p.bsk_bytes_fp64(),
-                     "key_stream_gbs": round(p.bsk_bytes_fp64() / (br_ms * 1e-3) / 1e9, 1)},
+                     "key_stream_gbs": round(p.bsk_bytes_fp64() / (br_ms * 1e-3) / 1e9, 1),
+                     "hbm_view": hbm_view(traffic, br_ms)},
         "kernels_ms": {"keyswitch": round(ks_ms, 3), "blind_rotate_extract": round(br_ms, 3)},
         "decrypt_errors": int(errors_max), "decrypt_checked": B * world,
         "output_noise_log2_std": round(noise_log2_std, 2),
@@ -536,6 +537,22 @@ def run_sweep(args, batches):
                     "outputs_equal": same, "speedup": round(plain_ms / tuned_ms, 3)})
     eng.close()
     return out
+
+
+def hbm_view(traffic, launch_ms):
+    """The same launch against the HBM roofline: DRAM bytes (ncu-derived,
+    scaled to the launch) per launch time over the measured copy bandwidth
+    of MEASURED_PEAKS.json."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if traffic is None or not os.path.exists(path):
+        return None
+    try:
+        peak = float(json.load(open(path))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return None
+    gbs = traffic / (launch_ms * 1e-3) / 1e9
+    return {"achieved_gbs": round(gbs, 1), "peak_gbs": peak, "frac": round(gbs / peak, 4),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"}
 
 
 def read_traffic(batch):
