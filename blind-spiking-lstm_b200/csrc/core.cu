@@ -218,10 +218,17 @@ struct BrShape {
 };
 
 static int max_smem_per_sm() {
-    int dev = 0, v = 0;
+    static int cached[64] = {0};
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    return v;
+    if (dev < 0 || dev >= 64) return 0;          // unknown: never place two CTAs per SM
+    if (!cached[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess || v <= 0)
+            v = 0;
+        cached[dev] = v > 0 ? v : -1;
+    }
+    return cached[dev] > 0 ? cached[dev] : 0;
 }
 
 
