@@ -27,7 +27,7 @@ namespace tfhe {
 constexpr int br_kt(int logn, int L) { return (L <= 3 && logn <= 11) ? 2 : 1; }
 
 struct BrArgs {
-    const double2* bsk;       // native [G][2][P][M][H]; reference layout (G,2,L,2,M,H)
+    const double2* bsk;       // native [G][2][P/2][M][H][2]; reference layout (G,2,L,2,M,H)
     const double2* all_rot;   // reference layout only: (2N, H)
     const double2* qt;
     const double2* tw;
@@ -56,6 +56,12 @@ struct BrArgs {
     long long wait_limit;     // clock cycles per mbarrier wait
     int* status;              // device status word (tfhe_device_status)
 };
+
+// the key words of digits 2j and 2j+1 of one slot: one 32-byte load (the
+// native key layout keeps them adjacent; p 32-byte aligned)
+__device__ __forceinline__ void ldg_pair(const double2* p, double2& x, double2& y) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(y.x), "=d"(y.y) : "l"(p));
+}
 
 // coefficient of X^e (any integer e) of a negacyclic polynomial in smem
 template <int LOGN>
@@ -350,22 +356,28 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                     double2 o0[KT], o1[KT];
     #pragma unroll
                     for (int kt = 0; kt < KT; ++kt) o0[kt] = o1[kt] = make_double2(0.0, 0.0);
-                    const double2* kb = args.bsk + gbase + jr;
+                    const double2* kb = args.bsk + gbase + jr;          // reference layout
+                    const double2* kb2 = args.bsk + gbase + 2 * (size_t)p; // native: pairs of digits
 #pragma unroll 1
                     for (int m = 0; m < M; ++m) {
                         if (args.prefetch > 0 || (args.prefetch < 0 && 2 * P * KT > 16)) {
                             // next pattern of this slot, or the first pattern of
                             // this thread's next slot: into L1 while this one computes
-                            const double2* nb = kb + (size_t)(m + 1) * H;
+                            const double2* nb = REFLAYOUT ? kb + (size_t)(m + 1) * H : kb2 + (size_t)(m + 1) * H * 2;
                             if (m + 1 == M) {
                                 const int tn = t + nt;
                                 const int pn = tn / KG;
-                                nb = (tn < KG * H) ? args.bsk + gbase + (REFLAYOUT ? 0 : pn) : nullptr;
+                                nb = (tn < KG * H) ? args.bsk + gbase + 2 * (size_t)pn : nullptr;
                                 if (REFLAYOUT) nb = nullptr;
                             }
                             if (nb) {
+                                if constexpr (REFLAYOUT) {
 #pragma unroll
-                                for (int bc = 0; bc < 2 * P; ++bc) prefetch_l1(nb + (size_t)bc * M * H);
+                                    for (int bc = 0; bc < 2 * P; ++bc) prefetch_l1(nb + (size_t)bc * M * H);
+                                } else {
+#pragma unroll
+                                    for (int j = 0; j < P; ++j) prefetch_l1(nb + (size_t)j * M * H * 2);
+                                }
                             }
                         }
                         double2 w[KT];
@@ -382,10 +394,18 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                         if constexpr (2 * P * KT <= 16) {
                             // both outputs' key words of this pattern in flight before use
                             double2 k0[P], k1[P];
+                            if constexpr (REFLAYOUT) {
 #pragma unroll
-                            for (int bc = 0; bc < P; ++bc) {
-                                k0[bc] = __ldg(kb + ((size_t)bc * M + m) * H);
-                                k1[bc] = __ldg(kb + ((size_t)(P + bc) * M + m) * H);
+                                for (int bc = 0; bc < P; ++bc) {
+                                    k0[bc] = __ldg(kb + ((size_t)bc * M + m) * H);
+                                    k1[bc] = __ldg(kb + ((size_t)(P + bc) * M + m) * H);
+                                }
+                            } else {
+#pragma unroll
+                                for (int j = 0; j < P / 2; ++j) {
+                                    ldg_pair(kb2 + ((size_t)j * M + m) * H * 2, k0[2 * j], k0[2 * j + 1]);
+                                    ldg_pair(kb2 + ((size_t)(P / 2 + j) * M + m) * H * 2, k1[2 * j], k1[2 * j + 1]);
+                                }
                             }
                             double2 t0[KT], t1[KT];
 #pragma unroll
@@ -409,8 +429,14 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 #pragma unroll
                             for (int a = 0; a < 2; ++a) {
                                 double2 kv[P];
+                                if constexpr (REFLAYOUT) {
 #pragma unroll
-                                for (int bc = 0; bc < P; ++bc) kv[bc] = __ldg(kb + ((size_t)(a * P + bc) * M + m) * H);
+                                    for (int bc = 0; bc < P; ++bc) kv[bc] = __ldg(kb + ((size_t)(a * P + bc) * M + m) * H);
+                                } else {
+#pragma unroll
+                                    for (int j = 0; j < P / 2; ++j)
+                                        ldg_pair(kb2 + ((size_t)(a * (P / 2) + j) * M + m) * H * 2, kv[2 * j], kv[2 * j + 1]);
+                                }
                                 double2 t[KT];
 #pragma unroll
                                 for (int kt = 0; kt < KT; ++kt) t[kt] = make_double2(0.0, 0.0);
@@ -520,7 +546,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 
 // ----------------------------------------------------------------------------
 // Forward FFT of the coefficient-domain bootstrapping key into the device
-// layout [G][2 out][P][M][H] (position order), P = 2L, bc = level * 2 + in.
+// layout [G][2 out][P/2][M][H][2] (position order; the two digits bc = 2j,
+// 2j+1 of a slot adjacent), P = 2L, bc = level * 2 + in.
 // Source: uint32 (2 in = left/right, 2 out = mask/body, G*M, L, N), the
 // layout of get_boostrapping_key_collapse (schemas/RLWE_jax.py:162-197).
 // The reference transforms the same integers with jax_fourier and permutes
@@ -533,7 +560,7 @@ struct BskConvArgs {
     const double2* tw;
     int G, M, L;
     long long npoly;   // 2 * 2 * G * M * L
-    int ring_nt;       // 0: [G][2][P][M][H]; > 0: [G][H/ring_nt][2][M][P][ring_nt]
+    int ring_nt;       // 0: [G][2][P/2][M][H][2]; > 0: [G][H/ring_nt][2][M][P][ring_nt]
 };
 
 template <int LOGN>
@@ -577,7 +604,7 @@ __global__ void __launch_bounds__(256) bsk_fft_kernel(const BskConvArgs a) {
             di = ((((size_t)g * parts + p / a.ring_nt) * 2 + out) * a.M + m) * P + bc;
             di = di * a.ring_nt + p % a.ring_nt;
         } else {
-            di = (((size_t)(g * 2 + out) * P + bc) * a.M + m) * H + p;
+            di = ((((size_t)(g * 2 + out) * (P / 2) + bc / 2) * a.M + m) * H + p) * 2 + (bc & 1);
         }
         a.dst[di] = buf[lp * H + swz(p)];
     }

@@ -21,7 +21,7 @@ struct tfhe_keys {
     tfhe_params p;
     int device = -1;
     int G = 0, M = 0;
-    double2* bsk = nullptr;     // [G][2][2L][M][N/2] FP64 Fourier, position order
+    double2* bsk = nullptr;     // [G][2][L][M][N/2][2] FP64 Fourier, position order
     uint32_t* ksk = nullptr;    // [n_big * l_ks][ldk]: columns 0..n-1 mask, n body
     int ldk = 0;
     const tfhe::FftPlan* plan = nullptr;
@@ -803,7 +803,7 @@ int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordere
     std::vector<double2> qt, tw;
     std::vector<uint16_t> freq;
     build_tables(N, qt, tw, freq);
-    // bsk_ordered (2 out, 2 in, L, G*M, H) at zeta^(2j+1) -> [G][2][P][M][H]
+    // bsk_ordered (2 out, 2 in, L, G*M, H) at zeta^(2j+1) -> [G][2][P/2][M][H][2]
     // at zeta^(4 freq[p] + 1) (the point or the conjugate of its partner)
     const size_t total = (size_t)G * 2 * P * M * H;
     std::vector<double2> host(total);
@@ -824,7 +824,7 @@ int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordere
                                 di = ((((size_t)g * (H / rnt) + pp / rnt) * 2 + a) * M + m) * P + bc;
                                 di = di * rnt + pp % rnt;
                             } else {
-                                di = ((((size_t)g * 2 + a) * P + bc) * M + m) * H + pp;
+                                di = (((((size_t)g * 2 + a) * (P / 2) + bc / 2) * M + m) * H + pp) * 2 + (bc & 1);
                             }
                             host[di] = e < N ? row[2 * j] : make_double2(row[N - 1 - 2 * j].x, -row[N - 1 - 2 * j].y);
                         }
