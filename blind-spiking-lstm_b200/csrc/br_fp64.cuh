@@ -63,6 +63,39 @@ __device__ __forceinline__ void ldg_pair(const double2* p, double2& x, double2& 
     asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(y.x), "=d"(y.y) : "l"(p));
 }
 
+// exp(-i pi n / 16), n = 1..7
+__device__ __forceinline__ double2 root32(int n) {
+    constexpr double C[8] = {1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+                             0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+                             0.19509032201612826785};
+    return make_double2(C[n], -C[8 - n]);
+}
+
+// The twist factors zeta^(n1 + (N/16) n2) = zeta^n1 exp(-i pi n2 / 16) and
+// the first superstage's twiddles W_H^(n1 k2) = (W_H^n1)^k2 (n2, k2 = 0..7)
+// of the butterfly a thread owns, from two table reads and 13 products
+// instead of 15 reads (a few ulp from the table values).  Where the root
+// table is in global memory (QTG) the reads are the costlier side: n=630
+// N=1024 went from 166.7 to 156.4 ms per 16384 ciphertexts; with the table in
+// shared memory (n=742 N=2048) the 52 extra FP64 instructions cost more
+// (280.7 -> 285.4 ms), so that layout keeps the reads.
+__device__ __forceinline__ void owned_factors(const double2* qt, const double2* tw, int n1, double2 (&wt)[8],
+                                              double2 (&w0)[8]) {
+    const double2 z = qt[n1];
+    wt[0] = z;
+#pragma unroll
+    for (int n2 = 1; n2 < 8; ++n2) wt[n2] = c_mul(z, root32(n2));
+    const double2 u = tw[n1];
+    w0[0] = make_double2(1.0, 0.0);
+    w0[1] = u;
+    w0[2] = c_mul(u, u);
+    w0[3] = c_mul(w0[2], u);
+    w0[4] = c_mul(w0[2], w0[2]);
+    w0[5] = c_mul(w0[4], u);
+    w0[6] = c_mul(w0[4], w0[2]);
+    w0[7] = c_mul(w0[4], w0[3]);
+}
+
 // coefficient of X^e (any integer e) of a negacyclic polynomial in smem
 template <int LOGN>
 __device__ __forceinline__ uint32_t ncoef(const uint32_t* p, int e) {
@@ -247,9 +280,14 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             }
             double2* pk = dec + (size_t)ok * P * H + oa * H;
             double2 w0[8];
-            w0[0] = make_double2(1.0, 0.0);
+            [[maybe_unused]] double2 wt[8];
+            if constexpr (QTG) {
+                owned_factors(qt, tw, on1, wt, w0);
+            } else {
+                w0[0] = make_double2(1.0, 0.0);
 #pragma unroll
-            for (int k2 = 1; k2 < 8; ++k2) w0[k2] = tw[(k2 - 1) * Q8 + on1];
+                for (int k2 = 1; k2 < 8; ++k2) w0[k2] = tw[(k2 - 1) * Q8 + on1];
+            }
 #pragma unroll
             for (int lvl = 0; lvl < L; ++lvl) {
                 double2 v[8];
@@ -261,7 +299,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                     const double yhi = x_hi[n2] * beta;
                     const double dhi = rint(yhi);
                     x_hi[n2] = yhi - dhi;
-                    const double2 w = qt[on1 + Q8 * n2];   // zeta^i
+                    const double2 w = QTG ? wt[n2] : qt[on1 + Q8 * n2];   // zeta^i
                     v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
                 }
                 dft8<false>(v);
@@ -472,11 +510,19 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             double2 v[8];
 #pragma unroll
             for (int k2 = 0; k2 < 8; ++k2) v[k2] = poly[swz(on1 + Q8 * k2)];
-            twiddle<8, Q8, true>(v, tw, on1);
+            [[maybe_unused]] double2 wt[8];
+            if constexpr (QTG) {
+                double2 w0[8];
+                owned_factors(qt, tw, on1, wt, w0);
+#pragma unroll
+                for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], c_conj(w0[k2]));
+            } else {
+                twiddle<8, Q8, true>(v, tw, on1);
+            }
             dft8<true>(v);
 #pragma unroll
             for (int n2 = 0; n2 < 8; ++n2) {
-                const double2 u = c_mul(c_conj(qt[on1 + Q8 * n2]), v[n2]);
+                const double2 u = c_mul(c_conj(QTG ? wt[n2] : qt[on1 + Q8 * n2]), v[n2]);
                 const double rlo = rint(u.x * inv_h);
                 const double rhi = rint(-u.y * inv_h);
                 acc_lo[n2] = rlo - q * rint(rlo * inv_q);
