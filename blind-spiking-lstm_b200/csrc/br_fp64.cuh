@@ -30,6 +30,7 @@ struct BrArgs {
     const double2* bsk;       // native [G][2][P/2][M][H][2]; reference layout (G,2,L,2,M,H)
     const double2* all_rot;   // reference layout only: (2N, H)
     const double2* qt;
+    const double2* qr;        // qt in rotation order (rot_slot): the QTG layout's only root table
     const double2* tw;
     const uint16_t* freq;
     int G, M, collapse, K;
@@ -79,9 +80,10 @@ __device__ __forceinline__ double2 root32(int n) {
 // N=1024 went from 166.7 to 156.4 ms per 16384 ciphertexts; with the table in
 // shared memory (n=742 N=2048) the 52 extra FP64 instructions cost more
 // (280.7 -> 285.4 ms), so that layout keeps the reads.
-__device__ __forceinline__ void owned_factors(const double2* qt, const double2* tw, int n1, double2 (&wt)[8],
+template <int LOGN>
+__device__ __forceinline__ void owned_factors(const double2* qr, const double2* tw, int n1, double2 (&wt)[8],
                                               double2 (&w0)[8]) {
-    const double2 z = qt[n1];
+    const double2 z = qr[rot_slot<LOGN>(n1)];
     wt[0] = z;
 #pragma unroll
     for (int n2 = 1; n2 < 8; ++n2) wt[n2] = c_mul(z, root32(n2));
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             double2 w0[8];
             [[maybe_unused]] double2 wt[8];
             if constexpr (QTG) {
-                owned_factors(qt, tw, on1, wt, w0);
+                owned_factors<LOGN>(args.qr, tw, on1, wt, w0);
             } else {
                 w0[0] = make_double2(1.0, 0.0);
 #pragma unroll
@@ -426,7 +428,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                                 w[kt] = __ldg(args.all_rot + (size_t)r * H + jr);
                                 if (cj) w[kt] = c_conj(w[kt]);
                             } else {
-                                w[kt] = root2n<LOGN>(qt, r * e);
+                                w[kt] = QTG ? root2n_rot<LOGN>(args.qr, r * e) : root2n<LOGN>(qt, r * e);
                             }
                         }
                         if constexpr (2 * P * KT <= 16) {
@@ -513,7 +515,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             [[maybe_unused]] double2 wt[8];
             if constexpr (QTG) {
                 double2 w0[8];
-                owned_factors(qt, tw, on1, wt, w0);
+                owned_factors<LOGN>(args.qr, tw, on1, wt, w0);
 #pragma unroll
                 for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], c_conj(w0[k2]));
             } else {

@@ -157,15 +157,21 @@ const FftPlan* get_plan(int N) {
     FftPlan* pl = new FftPlan();
     pl->N = N;
     pl->tw_count = (int)tw.size();
+    // rotation-order copy: root r at ((r mod N/8) << 2) | (r div N/8), as rot_slot
+    std::vector<double2> qr(qt.size());
+    for (int r = 0; r < N / 2; ++r) qr[((r % (N / 8)) << 2) | (r / (N / 8))] = qt[r];
     bool ok = cudaMalloc(&pl->qt, qt.size() * sizeof(double2)) == cudaSuccess &&
+              cudaMalloc(&pl->qr, qr.size() * sizeof(double2)) == cudaSuccess &&
               cudaMalloc(&pl->tw, tw.size() * sizeof(double2)) == cudaSuccess &&
               cudaMalloc(&pl->freq, freq.size() * sizeof(uint16_t)) == cudaSuccess &&
               cudaMemcpy(pl->qt, qt.data(), qt.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(pl->qr, qr.data(), qr.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(pl->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(pl->freq, freq.data(), freq.size() * sizeof(uint16_t), cudaMemcpyHostToDevice) == cudaSuccess;
     if (!ok) {
         set_error("FFT plan upload failed: " + std::string(cudaGetErrorString(cudaGetLastError())));
         cudaFree(pl->qt);
+        cudaFree(pl->qr);
         cudaFree(pl->tw);
         cudaFree(pl->freq);
         delete pl;
@@ -361,6 +367,7 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     const FftPlan* pl = get_plan(N);
     if (!pl) return TFHE_ERR_INTERNAL;
     args.qt = pl->qt;
+    args.qr = pl->qr;
     args.tw = pl->tw;
     args.freq = pl->freq;
     args.K = sh.K;

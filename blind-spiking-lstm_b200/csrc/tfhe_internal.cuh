@@ -110,6 +110,31 @@ __device__ __forceinline__ double2 root2n(const double2* qt, int idx) {
     return neg ? make_double2(-x, -y) : make_double2(x, y);
 }
 
+// Slot of root r in the rotation-order copy of the quarter table.  The X^r
+// factors one warp needs in the pointwise stage have table indices that
+// differ by multiples of N/8 (the slots' evaluation points differ in the last
+// superstage's digit), so r, r + N/8, r + N/4 and r + 3N/8 are stored side by
+// side: a warp's lookups then touch about two or three 128-byte lines instead
+// of five or six.
+template <int LOGN>
+__device__ __forceinline__ int rot_slot(int r) {
+    constexpr int E = (1 << LOGN) / 8;
+    return ((r & (E - 1)) << 2) | (r >> (LOGN - 3));
+}
+
+// root2n from the rotation-order table
+template <int LOGN>
+__device__ __forceinline__ double2 root2n_rot(const double2* qr, int idx) {
+    constexpr int N = 1 << LOGN;
+    idx &= (2 * N - 1);
+    const int quad = idx >> (LOGN - 1);
+    const double2 w = qr[rot_slot<LOGN>(idx & (N / 2 - 1))];
+    const bool odd = quad & 1, neg = quad & 2;
+    const double x = odd ? w.y : w.x;
+    const double y = odd ? -w.x : w.y;
+    return neg ? make_double2(-x, -y) : make_double2(x, y);
+}
+
 // ----------------------------------------------------------------------------
 // small DFTs in registers, natural order in and out
 // ----------------------------------------------------------------------------
@@ -395,6 +420,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 struct FftPlan {
     int N = 0;
     double2* qt = nullptr;     // N/2: exp(-i pi r / N)
+    double2* qr = nullptr;     // the same N/2 roots in rotation order (rot_slot)
     double2* tw = nullptr;     // Plan<LOGH>::TW per-stage twiddles
     uint16_t* freq = nullptr;  // H: frequency of each position
     int tw_count = 0;
