@@ -160,6 +160,11 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     double2* dec = reinterpret_cast<double2*>(smem_raw);           // K * P * H
     double2* qt_s = dec + (size_t)K * P * H;                        // N / 2 (unless QTG)
     const double2* qt = QTG ? args.qt : qt_s;
+    // root r of the quarter table: the shared copy is stored swizzled (qsw),
+    // which keeps the X^r lookups of the pointwise stage free of bank
+    // conflicts (n=742 N=2048: 280.3 -> 277.9 ms per 16384 ciphertexts,
+    // together with the level-fused prologue)
+    auto qtab = [&](int r) { return QTG ? qt[r] : qt[qsw<LOGN>(r)]; };
     double2* tw = QTG ? qt_s : qt_s + N / 2;                        // PL::TW
     uint16_t* freq = reinterpret_cast<uint16_t*>(tw + PL::TW);      // H
     int* rot = reinterpret_cast<int*>(freq + H);                    // K * M
@@ -177,7 +182,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     const long long my_sets = blockIdx.x < nsets ? (nsets - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
     if constexpr (!QTG)
-        for (int i = tid; i < N / 2; i += nt) qt_s[i] = args.qt[i];
+        for (int i = tid; i < N / 2; i += nt) qt_s[qsw<LOGN>(i)] = args.qt[i];
     for (int i = tid; i < PL::TW; i += nt) tw[i] = args.tw[i];
     for (int i = tid; i < H; i += nt) freq[i] = args.freq[i];
 
@@ -274,12 +279,6 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
         // prologue: gadget digits of the owned coefficients (float64 steps of
         // polynomial_jax.py:98-111), fold + twist, first DIF superstage
         {
-            double x_lo[8], x_hi[8];
-#pragma unroll
-            for (int n2 = 0; n2 < 8; ++n2) {
-                x_lo[n2] = acc_lo[n2] * inv_q;
-                x_hi[n2] = acc_hi[n2] * inv_q;
-            }
             double2* pk = dec + (size_t)ok * P * H + oa * H;
             double2 w0[8];
             [[maybe_unused]] double2 wt[8];
@@ -290,26 +289,64 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 #pragma unroll
                 for (int k2 = 1; k2 < 8; ++k2) w0[k2] = tw[(k2 - 1) * Q8 + on1];
             }
-#pragma unroll
-            for (int lvl = 0; lvl < L; ++lvl) {
-                double2 v[8];
+            if constexpr (!QTG && L <= 2) {
+                // all L digits of a coefficient pair at once, so its twist
+                // factor is read once per group rather than once per level
+                // (the same operations on every value as the level loop below)
+                double2 v[L][8];
 #pragma unroll
                 for (int n2 = 0; n2 < 8; ++n2) {
-                    const double ylo = x_lo[n2] * beta;
-                    const double dlo = rint(ylo);
-                    x_lo[n2] = ylo - dlo;
-                    const double yhi = x_hi[n2] * beta;
-                    const double dhi = rint(yhi);
-                    x_hi[n2] = yhi - dhi;
-                    const double2 w = QTG ? wt[n2] : qt[on1 + Q8 * n2];   // zeta^i
-                    v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
+                    double xlo = acc_lo[n2] * inv_q;
+                    double xhi = acc_hi[n2] * inv_q;
+                    const double2 w = qtab(on1 + Q8 * n2);   // zeta^i
+#pragma unroll
+                    for (int lvl = 0; lvl < L; ++lvl) {
+                        const double ylo = xlo * beta;
+                        const double dlo = rint(ylo);
+                        xlo = ylo - dlo;
+                        const double yhi = xhi * beta;
+                        const double dhi = rint(yhi);
+                        xhi = yhi - dhi;
+                        v[lvl][n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
+                    }
                 }
-                dft8<false>(v);
 #pragma unroll
-                for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
-                double2* poly = pk + lvl * 2 * H;
+                for (int lvl = 0; lvl < L; ++lvl) {
+                    dft8<false>(v[lvl]);
 #pragma unroll
-                for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[k2];
+                    for (int k2 = 1; k2 < 8; ++k2) v[lvl][k2] = c_mul(v[lvl][k2], w0[k2]);
+                    double2* poly = pk + lvl * 2 * H;
+#pragma unroll
+                    for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[lvl][k2];
+                }
+            } else {
+                double x_lo[8], x_hi[8];
+#pragma unroll
+                for (int n2 = 0; n2 < 8; ++n2) {
+                    x_lo[n2] = acc_lo[n2] * inv_q;
+                    x_hi[n2] = acc_hi[n2] * inv_q;
+                }
+#pragma unroll
+                for (int lvl = 0; lvl < L; ++lvl) {
+                    double2 v[8];
+#pragma unroll
+                    for (int n2 = 0; n2 < 8; ++n2) {
+                        const double ylo = x_lo[n2] * beta;
+                        const double dlo = rint(ylo);
+                        x_lo[n2] = ylo - dlo;
+                        const double yhi = x_hi[n2] * beta;
+                        const double dhi = rint(yhi);
+                        x_hi[n2] = yhi - dhi;
+                        const double2 w = QTG ? wt[n2] : qtab(on1 + Q8 * n2);   // zeta^i
+                        v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
+                    }
+                    dft8<false>(v);
+#pragma unroll
+                    for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
+                    double2* poly = pk + lvl * 2 * H;
+#pragma unroll
+                    for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[k2];
+                }
             }
         }
         __syncthreads();
@@ -353,7 +390,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                 }
 #pragma unroll
                 for (int kt = 0; kt < KR; ++kt) {
-                    const double2 w = root2n<LOGN>(qt, rot[kt * M + m] * e);
+                    const double2 w = root2n<LOGN, !QTG>(qt, rot[kt * M + m] * e);
                     if (a == 0) c_mac(o0[kt], w, t[kt]);
                     else c_mac(o1[kt], w, t[kt]);
                 }
@@ -428,7 +465,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                                 w[kt] = __ldg(args.all_rot + (size_t)r * H + jr);
                                 if (cj) w[kt] = c_conj(w[kt]);
                             } else {
-                                w[kt] = QTG ? root2n_rot<LOGN>(args.qr, r * e) : root2n<LOGN>(qt, r * e);
+                                w[kt] = QTG ? root2n_rot<LOGN>(args.qr, r * e) : root2n<LOGN, true>(qt, r * e);
                             }
                         }
                         if constexpr (2 * P * KT <= 16) {
@@ -524,7 +561,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             dft8<true>(v);
 #pragma unroll
             for (int n2 = 0; n2 < 8; ++n2) {
-                const double2 u = c_mul(c_conj(QTG ? wt[n2] : qt[on1 + Q8 * n2]), v[n2]);
+                const double2 u = c_mul(c_conj(QTG ? wt[n2] : qtab(on1 + Q8 * n2)), v[n2]);
                 const double rlo = rint(u.x * inv_h);
                 const double rhi = rint(-u.y * inv_h);
                 acc_lo[n2] = rlo - q * rint(rlo * inv_q);

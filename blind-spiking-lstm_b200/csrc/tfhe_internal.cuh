@@ -95,14 +95,24 @@ struct Plan {
 // stage take the minimum of 4 wavefronts per 32 16-byte requests.
 __device__ __forceinline__ int swz(int e) { return e ^ (((e >> 3) ^ (e >> 4)) & 7); }
 
-// exp(-i pi idx / N) for any idx, from the quarter table qt[r] =
-// exp(-i pi r / N), r in [0, N/2)
+// slot of root r in the swizzled shared-memory quarter table: the low three
+// bits (16-byte bank group) are XORed with bits 3.. and bits log2 N - 3..,
+// so both a warp's run of consecutive roots and the X^r lookups of one
+// pointwise pass (roots N/8 apart) fall in distinct bank groups
 template <int LOGN>
+__device__ __forceinline__ int qsw(int r) {
+    return r ^ (((r >> 3) ^ (r >> (LOGN - 3))) & 7);
+}
+
+// exp(-i pi idx / N) for any idx, from the quarter table qt[r] =
+// exp(-i pi r / N), r in [0, N/2) (stored at qsw(r) when SW)
+template <int LOGN, bool SW = false>
 __device__ __forceinline__ double2 root2n(const double2* qt, int idx) {
     constexpr int N = 1 << LOGN;
     idx &= (2 * N - 1);
     const int quad = idx >> (LOGN - 1);
-    const double2 w = qt[idx & (N / 2 - 1)];
+    const int r = idx & (N / 2 - 1);
+    const double2 w = qt[SW ? qsw<LOGN>(r) : r];
     // multiply by (-i)^quad with selects (lanes take different quadrants)
     const bool odd = quad & 1, neg = quad & 2;
     const double x = odd ? w.y : w.x;
