@@ -216,6 +216,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     const double q = ldexp(1.0, args.log2_q);
     const double inv_q = ldexp(1.0, -args.log2_q);
     const double beta = ldexp(1.0, args.log2_beta);
+    // q^-1 beta: the first level's beta acc / q in one (exact) product
+    const double inv_qb = ldexp(1.0, args.log2_beta - args.log2_q);
     constexpr double inv_h = 1.0 / H;
 
     for (long long iter = 0; iter < my_sets; ++iter) {
@@ -296,15 +298,14 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                 double2 v[L][8];
 #pragma unroll
                 for (int n2 = 0; n2 < 8; ++n2) {
-                    double xlo = acc_lo[n2] * inv_q;
-                    double xhi = acc_hi[n2] * inv_q;
+                    double xlo = 0.0, xhi = 0.0;
                     const double2 w = qtab(on1 + Q8 * n2);   // zeta^i
 #pragma unroll
                     for (int lvl = 0; lvl < L; ++lvl) {
-                        const double ylo = xlo * beta;
+                        const double ylo = lvl == 0 ? acc_lo[n2] * inv_qb : xlo * beta;
                         const double dlo = rint(ylo);
                         xlo = ylo - dlo;
-                        const double yhi = xhi * beta;
+                        const double yhi = lvl == 0 ? acc_hi[n2] * inv_qb : xhi * beta;
                         const double dhi = rint(yhi);
                         xhi = yhi - dhi;
                         v[lvl][n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
@@ -322,19 +323,14 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             } else {
                 double x_lo[8], x_hi[8];
 #pragma unroll
-                for (int n2 = 0; n2 < 8; ++n2) {
-                    x_lo[n2] = acc_lo[n2] * inv_q;
-                    x_hi[n2] = acc_hi[n2] * inv_q;
-                }
-#pragma unroll
                 for (int lvl = 0; lvl < L; ++lvl) {
                     double2 v[8];
 #pragma unroll
                     for (int n2 = 0; n2 < 8; ++n2) {
-                        const double ylo = x_lo[n2] * beta;
+                        const double ylo = lvl == 0 ? acc_lo[n2] * inv_qb : x_lo[n2] * beta;
                         const double dlo = rint(ylo);
                         x_lo[n2] = ylo - dlo;
-                        const double yhi = x_hi[n2] * beta;
+                        const double yhi = lvl == 0 ? acc_hi[n2] * inv_qb : x_hi[n2] * beta;
                         const double dhi = rint(yhi);
                         x_hi[n2] = yhi - dhi;
                         const double2 w = QTG ? wt[n2] : qtab(on1 + Q8 * n2);   // zeta^i
