@@ -352,6 +352,39 @@ def test_no_wait_timeouts_recorded():
     assert st.value == 0
 
 
+def test_two_cta_layout_matches_one_cta_layout_at_cfg1():
+    """At config 1, 296 ciphertexts (one wave of two per CTA) run two CTAs
+    per SM: root table in global memory in rotation order, twist factors
+    derived from one read.  One ciphertext per CTA runs the shared-memory
+    layout that the oracle tests above pin bit for bit; the two layouts must
+    agree bit for bit."""
+    name = "cfg1"
+    p = PARAMS[name]
+    eng = engine(name)
+    batch = 296
+    msgs, a, b = inputs(name, batch)
+    k, threads, smem = eng.launch_shape(batch)
+    # two CTAs per SM: K = 2 and no 8 KB root table in shared memory
+    assert k == 2 and threads == 2 * k * p["N"] // 16 and smem < 110 * 1024
+    lut = device_u32(np.stack([np.zeros(p["N"]), step_body(name)])[None])
+    two = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+    eng.set_tuning(ciphertexts_per_cta=1)
+    try:
+        assert eng.launch_shape(batch)[0] == 1
+        one = eng.pbs(device_u32(a), device_u32(b.reshape(-1)), lut)
+    finally:
+        eng.set_tuning()
+    assert torch.equal(two[0], one[0]) and torch.equal(two[1], one[1])
+    # and the first ciphertexts against the oracle directly
+    k4 = keys(name)
+    ca, cb = O.key_switch_LWE(k4.ksk, (a[:4], b[:4]), ks_params(name))
+    enc = [np.zeros((4, p["N"])), np.broadcast_to(step_body(name), (4, p["N"]))]
+    wa, wb = O.cuboot_merge((ca, cb), enc, k4.bsk_ordered, p["q"], p["beta_bs"], p["l_bs"], p["N"],
+                            p["collapse"], k4.all_rot, 1)
+    assert np.array_equal(host_u32(two[0])[:4], u32(wa))
+    assert np.array_equal(host_u32(two[1])[:4], u32(wb[..., 0]))
+
+
 def test_tuning_changes_speed_not_results(tmp_path):
     """Every launch shape gives identical outputs; the autotuner picks one,
     caches it and the cache is applied on the next call."""
