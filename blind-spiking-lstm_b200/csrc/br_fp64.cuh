@@ -26,6 +26,11 @@ namespace tfhe {
 // CTA's ciphertext count K is always a multiple of it (launcher)
 constexpr int br_kt(int logn, int L) { return (L <= 3 && logn <= 11) ? 2 : 1; }
 
+// whether small-K launches of the one-CTA layout get extra threads (the XT
+// kernels, instantiated for L <= 2; at L >= 3 the ownership guard costs
+// registers and spills, so those shapes launch exactly the owners)
+constexpr bool br_extra_threads(int L) { return L <= 2; }
+
 struct BrArgs {
     const double2* bsk;       // native [G][2][P/2][M][H][2]; reference layout (G,2,L,2,M,H)
     const double2* all_rot;   // reference layout only: (2N, H)
@@ -144,7 +149,8 @@ __device__ __forceinline__ void forward_middle(double2* dec, int npoly, const do
 // chunk of P * NT words is contiguous (NT = KR H / 4 = threads per CTA).
 // QTG: the quarter root table is read from global memory (L1-cached) instead
 // of shared memory, so two CTAs of half the ciphertexts fit on one SM.
-template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP, bool QTG = false>
+// XT: the CTA may have more threads than the 2 K N/16 butterfly owners.
+template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP, bool QTG = false, bool XT = false>
 __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp64_kernel(const BrArgs args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
@@ -209,9 +215,15 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
     }
 
     // the butterfly this thread owns in the first / last superstage
-    const int ok = tid / (2 * Q8);
-    const int oa = (tid / Q8) & 1;
-    const int on1 = tid % Q8;
+    // a CTA may have more threads than owned butterflies (2 K N/16): the
+    // others shadow an owner's butterfly in the register-resident
+    // superstages without storing anything, and share the shared-memory
+    // superstages and the pointwise stage
+    const bool owner = !XT || tid < 2 * K * Q8;
+    const int otid = owner ? tid : tid % (2 * K * Q8);
+    const int ok = otid / (2 * Q8);
+    const int oa = (otid / Q8) & 1;
+    const int on1 = otid % Q8;
 
     const double q = ldexp(1.0, args.log2_q);
     const double inv_q = ldexp(1.0, -args.log2_q);
@@ -318,7 +330,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                     for (int k2 = 1; k2 < 8; ++k2) v[lvl][k2] = c_mul(v[lvl][k2], w0[k2]);
                     double2* poly = pk + lvl * 2 * H;
 #pragma unroll
-                    for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[lvl][k2];
+                    for (int k2 = 0; k2 < 8; ++k2)
+                        if (owner) poly[swz(on1 + Q8 * k2)] = v[lvl][k2];
                 }
             } else {
                 double x_lo[8], x_hi[8];
@@ -341,7 +354,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                     for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
                     double2* poly = pk + lvl * 2 * H;
 #pragma unroll
-                    for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[k2];
+                    for (int k2 = 0; k2 < 8; ++k2)
+                        if (owner) poly[swz(on1 + Q8 * k2)] = v[k2];
                 }
             }
         }
@@ -569,7 +583,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 
     // ---------------------------------------------------------------- epilogue
     if constexpr (REFLAYOUT) {
-        if (ct0 + ok < args.B) {
+        if (owner && ct0 + ok < args.B) {
             int64_t* dst = args.out_i64 + (ct0 + ok) * 2 * N + oa * N;
 #pragma unroll
             for (int n2 = 0; n2 < 8; ++n2) {
@@ -581,7 +595,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
         // ACC to shared memory as u32, then rotate by -b~ (RLWE_jax.py:295-297)
         // and, for the PBS, extract n_lut LWEs (RLWE_jax.py:301-303)
         uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);       // [K][2][N]
-        {
+        if (owner) {
             uint32_t* dst = acc + (size_t)ok * 2 * N + oa * N;
 #pragma unroll
             for (int n2 = 0; n2 < 8; ++n2) {

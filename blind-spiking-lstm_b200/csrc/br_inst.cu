@@ -12,7 +12,24 @@
 
 namespace tfhe {
 
-BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt, bool qtg) {
+BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt, bool qtg, bool xt) {
+    // the extra-thread kernels: one-CTA layout, L <= 2
+    if (xt) {
+        if (kr != 0 || qtg) return nullptr;
+        switch (L) {
+            case 1:
+                if (reflayout) return kt == 2 ? br_fp64_kernel<BR_LOGN, 1, true, 0, 2, false, true>
+                                              : br_fp64_kernel<BR_LOGN, 1, true, 0, 1, false, true>;
+                return kt == 2 ? br_fp64_kernel<BR_LOGN, 1, false, 0, 2, false, true>
+                               : br_fp64_kernel<BR_LOGN, 1, false, 0, 1, false, true>;
+            case 2:
+                if (reflayout) return kt == 2 ? br_fp64_kernel<BR_LOGN, 2, true, 0, 2, false, true>
+                                              : br_fp64_kernel<BR_LOGN, 2, true, 0, 1, false, true>;
+                return kt == 2 ? br_fp64_kernel<BR_LOGN, 2, false, 0, 2, false, true>
+                               : br_fp64_kernel<BR_LOGN, 2, false, 0, 1, false, true>;
+            default: return nullptr;
+        }
+    }
 #define TFHE_BR_CASE(LL)                                                                         \
     case LL:                                                                                     \
         if (reflayout) return kt == 2 ? br_fp64_kernel<BR_LOGN, LL, true, 0, 2>                    \

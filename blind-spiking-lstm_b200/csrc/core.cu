@@ -221,6 +221,7 @@ struct BrShape {
     int kr = 0, stages = 0;   // key ring (kr > 0)
     int kt = 1;               // ciphertexts per thread in the pointwise stage
     bool qtg = false;         // quarter root table in global memory (two CTAs per SM)
+    bool xt = false;          // more threads than butterfly owners (XT kernels)
 };
 
 static int max_smem_per_sm() {
@@ -272,20 +273,29 @@ static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0, boo
         const size_t smem = per_ct * K + br_table_bytes(N) + (size_t)(K * M + K) * sizeof(int) + 16;
         if (smem <= limit) {
             s.K = K;
-            s.nt = K * 2 * Q8;
+            // 2 K N/16 threads own the butterflies of the register-resident
+            // superstages; where the kernel allows extra threads they make it
+            // 512 whatever K is, all of them sharing the shared-memory
+            // superstages and the pointwise stage, so a batch under one wave
+            // (small K) still runs 16 warps per SM
+            s.nt = br_extra_threads(L) ? std::max(K * 2 * Q8, 512) : K * 2 * Q8;
+            s.xt = s.nt > K * 2 * Q8;
             s.smem = smem;
             s.kt = (K % KT == 0) ? KT : 1;
             // two CTAs per SM where they fit once the quarter root table is
             // read from global memory (automatic shapes halve K for it): their
             // phases drift apart, so one CTA's FFT overlaps the other's key
             // loads (n=630 N=1024: 181.2 -> 166.8 ms per 16384 ciphertexts)
-            if (allow_qtg && s.kt == 2) {
+            // (only for batches beyond one CTA per SM: below that the one-CTA
+            // layout of 512 threads is the faster of the two)
+            if (allow_qtg && s.kt == 2 && B > (long long)K * std::max(1, sm_count())) {
                 const int K2 = (kreq <= 0 && K % 4 == 0) ? K / 2 : K;
                 const size_t smem2 = per_ct * K2 + br_table_bytes(N) - (size_t)(N / 2) * sizeof(double2) +
                                      (size_t)(K2 * M + K2) * sizeof(int) + 16;
                 if (2 * (smem2 + 1024) <= (size_t)max_smem_per_sm()) {
                     s.K = K2;
                     s.nt = K2 * 2 * Q8;
+                    s.xt = false;
                     s.smem = smem2;
                     s.kt = 2;
                     s.qtg = true;
@@ -358,7 +368,7 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
                               : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0, !reflayout);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
-    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt, sh.qtg);
+    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt, sh.qtg, sh.xt);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
     if (sh.K < 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT,

@@ -10,7 +10,7 @@ using BrKernel = void (*)(const BrArgs);
 using BrConvKernel = void (*)(const BskConvArgs);
 
 #define TFHE_DECLARE_LOGN(LG)                              \
-    BrKernel br_fp64_logn_##LG(int L, bool reflayout, int kr, int kt, bool qtg);     \
+    BrKernel br_fp64_logn_##LG(int L, bool reflayout, int kr, int kt, bool qtg, bool xt);     \
     BrConvKernel bsk_fft_logn_##LG();
 
 TFHE_DECLARE_LOGN(7)
@@ -21,14 +21,15 @@ TFHE_DECLARE_LOGN(11)
 TFHE_DECLARE_LOGN(12)
 #undef TFHE_DECLARE_LOGN
 
-inline BrKernel br_fp64_kernel_for(int logn, int L, bool reflayout, int kr, int kt, bool qtg = false) {
+inline BrKernel br_fp64_kernel_for(int logn, int L, bool reflayout, int kr, int kt, bool qtg = false,
+                                   bool xt = false) {
     switch (logn) {
-        case 7: return br_fp64_logn_7(L, reflayout, kr, kt, qtg);
-        case 8: return br_fp64_logn_8(L, reflayout, kr, kt, qtg);
-        case 9: return br_fp64_logn_9(L, reflayout, kr, kt, qtg);
-        case 10: return br_fp64_logn_10(L, reflayout, kr, kt, qtg);
-        case 11: return br_fp64_logn_11(L, reflayout, kr, kt, qtg);
-        case 12: return br_fp64_logn_12(L, reflayout, kr, kt, qtg);
+        case 7: return br_fp64_logn_7(L, reflayout, kr, kt, qtg, xt);
+        case 8: return br_fp64_logn_8(L, reflayout, kr, kt, qtg, xt);
+        case 9: return br_fp64_logn_9(L, reflayout, kr, kt, qtg, xt);
+        case 10: return br_fp64_logn_10(L, reflayout, kr, kt, qtg, xt);
+        case 11: return br_fp64_logn_11(L, reflayout, kr, kt, qtg, xt);
+        case 12: return br_fp64_logn_12(L, reflayout, kr, kt, qtg, xt);
         default: return nullptr;
     }
 }

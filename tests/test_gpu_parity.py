@@ -353,7 +353,7 @@ def test_no_wait_timeouts_recorded():
 
 
 def test_two_cta_layout_matches_one_cta_layout_at_cfg1():
-    """At config 1, 296 ciphertexts (one wave of two per CTA) run two CTAs
+    """At config 1, 1184 ciphertexts (two waves of two per CTA) run two CTAs
     per SM: root table in global memory in rotation order, twist factors
     derived from one read.  One ciphertext per CTA runs the shared-memory
     layout that the oracle tests above pin bit for bit; the two layouts must
@@ -361,7 +361,7 @@ def test_two_cta_layout_matches_one_cta_layout_at_cfg1():
     name = "cfg1"
     p = PARAMS[name]
     eng = engine(name)
-    batch = 296
+    batch = 1184
     msgs, a, b = inputs(name, batch)
     k, threads, smem = eng.launch_shape(batch)
     # two CTAs per SM: K = 2 and no 8 KB root table in shared memory
