@@ -29,7 +29,7 @@ constexpr int br_kt(int logn, int L) { return (L <= 3 && logn <= 11) ? 2 : 1; }
 // whether small-K launches of the one-CTA layout get extra threads (the XT
 // kernels, instantiated for L <= 2; at L >= 3 the ownership guard costs
 // registers and spills, so those shapes launch exactly the owners)
-constexpr bool br_extra_threads(int L) { return L <= 2; }
+constexpr bool br_extra_threads(int L) { return L <= 3; }
 
 struct BrArgs {
     const double2* bsk;       // native [G][2][P/2][M][H][2]; reference layout (G,2,L,2,M,H)

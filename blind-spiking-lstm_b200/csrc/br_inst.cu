@@ -27,6 +27,11 @@ BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt,
                                               : br_fp64_kernel<BR_LOGN, 2, true, 0, 1, false, true>;
                 return kt == 2 ? br_fp64_kernel<BR_LOGN, 2, false, 0, 2, false, true>
                                : br_fp64_kernel<BR_LOGN, 2, false, 0, 1, false, true>;
+            case 3:
+                if (reflayout) return kt == 2 ? br_fp64_kernel<BR_LOGN, 3, true, 0, 2, false, true>
+                                              : br_fp64_kernel<BR_LOGN, 3, true, 0, 1, false, true>;
+                return kt == 2 ? br_fp64_kernel<BR_LOGN, 3, false, 0, 2, false, true>
+                               : br_fp64_kernel<BR_LOGN, 3, false, 0, 1, false, true>;
             default: return nullptr;
         }
     }
