@@ -385,6 +385,20 @@ def test_two_cta_layout_matches_one_cta_layout_at_cfg1():
     assert np.array_equal(host_u32(two[1])[:4], u32(wb[..., 0]))
 
 
+@pytest.mark.parametrize("name", ["cfg1", "cfg2"])
+def test_small_batches_get_512_threads(name):
+    """Under one wave, a CTA holds K < max ciphertexts but still 512 threads:
+    2K N/16 own the register-resident butterflies, the rest share the
+    shared-memory stages (the bit-exact tests above run these shapes)."""
+    p = PARAMS[name]
+    eng = engine(name)
+    for batch in (1, 100):
+        k, threads, smem = eng.launch_shape(batch)
+        assert k == 1 and threads == 512 and 2 * k * p["N"] // 16 < threads
+    k, threads, smem = eng.launch_shape(16384)
+    assert threads == 2 * k * p["N"] // 16
+
+
 def test_tuning_changes_speed_not_results(tmp_path):
     """Every launch shape gives identical outputs; the autotuner picks one,
     caches it and the cache is applied on the next call."""
