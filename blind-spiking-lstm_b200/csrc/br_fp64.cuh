@@ -9,13 +9,13 @@
 // reduction are the reference's float64 operations, so every stage but the
 // FFT rounding is bit-identical; with |FFT error| < 1/2 the products are too.
 //
-// Work mapping (NT = 2 K H/8 threads):
-//  * each thread owns one radix-8 butterfly (k, a, n1) of the first forward /
-//    last inverse superstage and keeps ACC[k][a][n1 + (H/8) n2] and
+// Work mapping (2 K H/8 butterfly owners; XT kernels run 512 threads):
+//  * each owner thread has one radix-8 butterfly (k, a, n1) of the first
+//    forward / last inverse superstage and keeps ACC[k][a][n1 + (H/8) n2] and
 //    ACC[k][a][n1 + (H/8) n2 + H] (n2 < 8) in registers across groups;
 //  * middle superstages run over all polynomials in shared memory;
-//  * the pointwise stage maps lanes to (slot p, ciphertext k) with k fastest,
-//    so the K lanes of one slot load the same key word in one request.
+//  * the pointwise stage gives each thread one slot p for KT ciphertexts, so
+//    every key word a thread loads serves KT ciphertexts.
 #pragma once
 
 #include "tfhe_internal.cuh"
