@@ -155,7 +155,7 @@ def run_engine(args, rank, world, local_rank, dist):
     import numpy as np
     import torch
     from tfhe_b200 import client
-    from tfhe_b200.engine import Keys, probe_fp64_peak
+    from tfhe_b200.engine import Keys, launch_count, probe_fp64_peak
     from tfhe_b200.params import CONFIG1, CONFIG2
 
     torch.cuda.set_device(local_rank)
@@ -198,10 +198,12 @@ def run_engine(args, rank, world, local_rank, dist):
     clocks.start()
     barrier()
     torch.cuda.synchronize()
+    n_launch0 = launch_count()
     t0.record(stream)
     for s in range(args.steps):
         step_device(evs[s])
     t1.record(stream)
+    gpu_launches = launch_count() - n_launch0
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
@@ -279,7 +281,7 @@ def run_engine(args, rank, world, local_rank, dist):
         "kernels_ms": {"keyswitch": round(ks_ms, 3), "blind_rotate_extract": round(br_ms, 3)},
         "decrypt_errors": int(errors_max), "decrypt_checked": B * world,
         "output_noise_log2_std": round(noise_log2_std, 2),
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": gpu_launches,
         "clocks": clk,
     }
     return line
@@ -296,6 +298,7 @@ def run_lstm(args):
     import numpy as np
     import torch
     from tfhe_b200 import spike_model as SM
+    from tfhe_b200.engine import launch_count
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
@@ -328,10 +331,12 @@ def run_lstm(args):
     clocks = ClockSampler(0)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_launch0 = launch_count()
     e0.record(stream)
     for _ in range(args.steps):
         la, lb = forward(xs_d)
     e1.record(stream)
+    gpu_launches = launch_count() - n_launch0
     torch.cuda.synchronize()
     dev_ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
@@ -351,7 +356,6 @@ def run_lstm(args):
 
     logits = SM.decrypt_logits(model, la_h, lb_h)
     plain, _ = SM.plain_forward(model, tokens)
-    per_step = 21 * cfg.layers
     pbs_per_seq = args.seq_len * cfg.layers * 3 * (cfg.hidden // cfg.n_lut) + cfg.hidden
     return {"metric": "encrypted Spike-LSTM sequences/s (layer + head)", "value": round(args.seqs / dev_ms * 1e3, 3),
             "unit": "seq/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -364,7 +368,7 @@ def run_lstm(args):
             "e2e": {"value": round(args.seqs / e2e_ms * 1e3, 3), "unit": "seq/s",
                     "h2d_bytes_per_step": int(xs_h.numel() * 4), "d2h_bytes_per_step": int((la.numel() + lb.numel()) * 4)},
             "pbs_per_sequence": pbs_per_seq, "pbs_per_s": round(pbs_per_seq * args.seqs / dev_ms * 1e3, 1),
-            "gpu_launches": args.steps * (per_step * args.seq_len + 6),
+            "gpu_launches": gpu_launches,
             "decrypted_logits": [round(float(v), 2) for v in logits[:8]],
             "plain_logits": [round(float(v), 2) for v in plain[:8]],
             "logit_sign_agreement": float(np.mean(np.sign(logits) == np.sign(plain))),

@@ -228,6 +228,7 @@ static int launch_l(const KsTcArgs& args, cudaStream_t stream) {
         cudaFuncSetAttribute(ks_tc_kernel<L, PACK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "tensor-core contraction attribute");
     const dim3 grid((unsigned)(args.npad / KTC_N), (unsigned)((args.B + KTC_M - 1) / KTC_M));
+    count_launch();
     ks_tc_kernel<L, PACK><<<grid, KTC_THREADS, smem, stream>>>(args);
     return check_cuda(cudaGetLastError(), "tensor-core contraction launch");
 }
@@ -282,6 +283,7 @@ __global__ void packing_limbs_kernel(const uint32_t* __restrict__ ksp, int n_dim
 int build_packing_limbs(const uint32_t* ksp, int n_dim, int l, int N, int8_t* limbs, cudaStream_t stream) {
     const long long total = 2LL * N * n_dim * l;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+    count_launch();
     packing_limbs_kernel<<<blocks, 256, 0, stream>>>(ksp, n_dim, l, N, limbs);
     return check_cuda(cudaGetLastError(), "packing limb launch");
 }

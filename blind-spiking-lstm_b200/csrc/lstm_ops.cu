@@ -500,6 +500,7 @@ int launch_trace(const TraceArgs& a, long long R, size_t smem, cudaStream_t stre
     auto kern = trace_pack_kernel<LOGN>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return check_cuda(cudaGetLastError(), "trace kernel attribute");
+    count_launch();
     kern<<<(unsigned)R, 256, smem, stream>>>(a);
     return check_cuda(cudaGetLastError(), "trace kernel launch");
 }
@@ -507,6 +508,7 @@ int launch_trace(const TraceArgs& a, long long R, size_t smem, cudaStream_t stre
 template <int LOGN>
 int launch_poly_fft(const uint32_t* src, long long npoly, const FftPlan* pl, double2* dst, cudaStream_t stream) {
     const size_t smem = (size_t)(1 << (LOGN - 1)) * sizeof(double2);
+    count_launch();
     poly_fft_kernel<LOGN><<<(unsigned)npoly, 256, smem, stream>>>(src, npoly, pl->qt, pl->tw, dst);
     return check_cuda(cudaGetLastError(), "polynomial FFT launch");
 }
@@ -553,6 +555,7 @@ int tfhe_linear_extract(const int32_t* weights, const int32_t* bias, int32_t J, 
         cudaSuccess)
         return check_cuda(cudaGetLastError(), "linear kernel attribute");
     const dim3 grid((J + LIN_JT - 1) / LIN_JT, (unsigned)S);
+    count_launch();
     linear_extract_kernel<<<grid, LIN_NT, smem, (cudaStream_t)stream>>>(weights, bias, J, rlwe, N, out_a, out_b);
     return check_cuda(cudaGetLastError(), "linear kernel launch");
 }
@@ -569,6 +572,7 @@ int tfhe_lut_mul_sum(const int32_t* luts, int32_t groups, int32_t per_group, con
         cudaSuccess)
         return check_cuda(cudaGetLastError(), "lut product attribute");
     const dim3 grid((unsigned)per_group, (unsigned)S);
+    count_launch();
     lut_mul_sum_kernel<<<grid, LM_NT, smem, (cudaStream_t)stream>>>(luts, groups, per_group, rlwe, N, out);
     return check_cuda(cudaGetLastError(), "lut product launch");
 }
@@ -636,6 +640,7 @@ int tfhe_pack_lwes(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_b
     if (S == 0) return TFHE_OK;
     if (!ksp || !out || (T > 0 && (!lwe_a || !lwe_b))) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: null pointer");
     const long long total = S * 2 * (long long)N;
+    count_launch();
     pack_init_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(lwe_b, T, S, N, out);
     const int rc = check_cuda(cudaGetLastError(), "packing init launch");
     if (rc != TFHE_OK) return rc;
@@ -643,6 +648,7 @@ int tfhe_pack_lwes(const uint32_t* ksp, int32_t n_dim, int32_t N, int32_t log2_b
     const long long rows = S * T;
     if ((rows + PK_TB - 1) / PK_TB > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: too many LWEs per call");
     const dim3 grid((2 * N + PK_TO - 1) / PK_TO, (unsigned)((rows + PK_TB - 1) / PK_TB));
+    count_launch();
     pack_ks_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(lwe_a, n_dim, T, S, ksp, N, l, log2_beta, out);
     return check_cuda(cudaGetLastError(), "packing launch");
 }
@@ -707,6 +713,7 @@ int tfhe_pack_lwes_with_key(const tfhe_packing_key* key, const uint32_t* lwe_a, 
     if (S == 0) return TFHE_OK;
     if (!lwe_a || !lwe_b || !out) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing: null pointer");
     const long long total = S * 2 * (long long)N;
+    count_launch();
     pack_init_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(lwe_b, T, S, N, out);
     const int rc = check_cuda(cudaGetLastError(), "packing init launch");
     if (rc != TFHE_OK) return rc;
@@ -724,6 +731,7 @@ int tfhe_rlwe_rotate_add(const uint32_t* x, int32_t rot, const uint32_t* y, int6
     if (x == out && rot % (2 * N) != 0)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "rotate/add: out may not alias x when rotating");
     const int r = ((rot % (2 * N)) + 2 * N) % (2 * N);
+    count_launch();
     rlwe_rotate_add_kernel<<<grid_for(S * 2 * (long long)N), 256, 0, (cudaStream_t)stream>>>(x, r, y, S, N, out);
     return check_cuda(cudaGetLastError(), "rotate/add launch");
 }
@@ -732,6 +740,7 @@ int tfhe_u32_add(const uint32_t* x, const uint32_t* y, int64_t n, uint32_t* out,
     if (n < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "add: negative count");
     if (n == 0) return TFHE_OK;
     if (!x || !y || !out) return fail(TFHE_ERR_INVALID_ARGUMENT, "add: null pointer");
+    count_launch();
     u32_add_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(x, y, n, out);
     return check_cuda(cudaGetLastError(), "add launch");
 }

@@ -27,6 +27,8 @@ namespace tfhe {
 void set_error(const std::string& msg);
 // the per-device word kernels set on a bounded-wait timeout (tfhe_device_status)
 int* device_status_word();
+// counts one kernel launch by this library (tfhe_launch_count)
+void count_launch();
 // bound of every mbarrier wait, in clock cycles (about 2 s)
 constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL;
 int fail(int code, const std::string& msg);

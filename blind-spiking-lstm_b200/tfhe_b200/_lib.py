@@ -57,6 +57,7 @@ SIGNATURES = {
     "tfhe_cuboot_merge": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _P]),
     "tfhe_probe_fp64_fma": (ctypes.c_int, [_I32, _I32, _I32, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "tfhe_device_status": (ctypes.c_int, [ctypes.POINTER(_I32), _I32]),
+    "tfhe_launch_count": (ctypes.c_int64, []),
     "tfhe_probe_wait_timeout": (ctypes.c_int, [_I64, ctypes.POINTER(_I32)]),
     "tfhe_keyswitch_ref": (ctypes.c_int, [_P, _P, _P, _P, _I32, _I32, _I32, _I32, _P, _P, _I64, _P]),
     "tfhe_pbs_host": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _I64, _P]),

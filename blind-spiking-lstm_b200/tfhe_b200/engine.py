@@ -234,6 +234,12 @@ def sample_extract(acc, n_lut=1, out_a=None, out_b=None, stream=None):
     return out_a, out_b
 
 
+def launch_count() -> int:
+    """Kernels the library has launched in this process (tfhe_launch_count);
+    the difference across a region of calls counts that region's launches."""
+    return int(_lib.load().tfhe_launch_count())
+
+
 def probe_fp64_peak(iters=4096, reps=5) -> float:
     """Measured FP64 FMA throughput of the current device in TFLOP/s (best
     of ``reps`` launches of 8 independent FMA chains per thread, 8 CTAs of

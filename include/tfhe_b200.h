@@ -200,6 +200,11 @@ int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int3
 #define TFHE_DEVICE_TIMEOUT 1
 int tfhe_device_status(int32_t* status_out, int32_t clear);
 
+/* Kernels this library has launched in this process, all devices (no
+ * counterpart in the reference): the difference across a region of calls is
+ * the number of the library's kernel launches in it. */
+int64_t tfhe_launch_count(void);
+
 /* Diagnostics (no counterpart in the reference): runs one bounded mbarrier
  * wait that nothing completes, with a limit of limit_cycles clock cycles;
  * *waited_out = 0 when it gave up (the device status then reads

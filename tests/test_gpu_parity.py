@@ -385,6 +385,33 @@ def test_two_cta_layout_matches_one_cta_layout_at_cfg1():
     assert np.array_equal(host_u32(two[1])[:4], u32(wb[..., 0]))
 
 
+def test_partial_last_round_runs_as_its_own_launch():
+    """n=742 N=2048, 396 ciphertexts: two full rounds of K = 2 on 148 CTAs,
+    then the last 100 as a second launch of one ciphertext per CTA; the
+    outputs equal one launch of the requested K = 2 bit for bit, and the
+    library's launch counter sees the two launches."""
+    from tfhe_b200.engine import launch_count
+    name = "cfg2"
+    p = PARAMS[name]
+    eng = engine(name)
+    batch = 396
+    msgs, a, b = inputs(name, batch, t=16)
+    lut = device_u32(np.stack([np.zeros(p["N"]), step_body(name, t=16)])[None])
+    ka, kb = eng.keyswitch(device_u32(a), device_u32(b.reshape(-1)))
+    n0 = launch_count()
+    split = eng.blind_rotate(ka, kb, lut)
+    n_split = launch_count() - n0
+    eng.set_tuning(ciphertexts_per_cta=2)
+    try:
+        n0 = launch_count()
+        one = eng.blind_rotate(ka, kb, lut)
+        n_one = launch_count() - n0
+    finally:
+        eng.set_tuning()
+    assert torch.equal(split, one)
+    assert n_split == n_one + 1
+
+
 @pytest.mark.parametrize("name", ["cfg1", "cfg2"])
 def test_small_batches_get_512_threads(name):
     """Under one wave, a CTA holds K < max ciphertexts but still 512 threads:
