@@ -27,8 +27,7 @@ namespace tfhe {
 constexpr int br_kt(int logn, int L) { return (L <= 3 && logn <= 11) ? 2 : 1; }
 
 // whether small-K launches of the one-CTA layout get extra threads (the XT
-// kernels, instantiated for L <= 2; at L >= 3 the ownership guard costs
-// registers and spills, so those shapes launch exactly the owners)
+// kernels, instantiated for L <= 3; larger L launch exactly the owners)
 constexpr bool br_extra_threads(int L) { return L <= 3; }
 
 struct BrArgs {
@@ -572,8 +571,16 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 #pragma unroll
             for (int n2 = 0; n2 < 8; ++n2) {
                 const double2 u = c_mul(c_conj(QTG ? wt[n2] : qtab(on1 + Q8 * n2)), v[n2]);
-                const double rlo = rint(u.x * inv_h);
-                const double rhi = rint(-u.y * inv_h);
+                // the native key is stored times 1/H (bsk_fft_kernel), which
+                // already applied the inverse transform's 1/H, exactly
+                double rlo, rhi;
+                if constexpr (REFLAYOUT) {
+                    rlo = rint(u.x * inv_h);
+                    rhi = rint(-u.y * inv_h);
+                } else {
+                    rlo = rint(u.x);
+                    rhi = rint(-u.y);
+                }
                 acc_lo[n2] = rlo - q * rint(rlo * inv_q);
                 acc_hi[n2] = rhi - q * rint(rhi * inv_q);
             }
@@ -701,7 +708,11 @@ __global__ void __launch_bounds__(256) bsk_fft_kernel(const BskConvArgs a) {
         } else {
             di = ((((size_t)(g * 2 + out) * (P / 2) + bc / 2) * a.M + m) * H + p) * 2 + (bc & 1);
         }
-        a.dst[di] = buf[lp * H + swz(p)];
+        // times 1/H: a power of two, so every product and sum of the blind
+        // rotation comes out exactly 1/H times the unscaled one, and the
+        // inverse transform's 1/H needs no multiply of its own
+        const double2 v = buf[lp * H + swz(p)];
+        a.dst[di] = make_double2(v.x * (1.0 / H), v.y * (1.0 / H));
     }
 }
 

@@ -879,7 +879,9 @@ int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordere
                             } else {
                                 di = (((((size_t)g * 2 + a) * (P / 2) + bc / 2) * M + m) * H + pp) * 2 + (bc & 1);
                             }
-                            host[di] = e < N ? row[2 * j] : make_double2(row[N - 1 - 2 * j].x, -row[N - 1 - 2 * j].y);
+                            // times 1/H, as bsk_fft_kernel stores the native key
+                            const double2 w = e < N ? row[2 * j] : make_double2(row[N - 1 - 2 * j].x, -row[N - 1 - 2 * j].y);
+                            host[di] = make_double2(w.x / H, w.y / H);
                         }
                     }
     int rc = check_cuda(cudaMalloc(&k->bsk, total * sizeof(double2)), "cudaMalloc(bsk)");
