@@ -28,7 +28,7 @@ struct tfhe_keys {
     const tfhe::FftPlan* plan = nullptr;
     int64_t bytes = 0;
     int ring_kr = 0;            // > 0: key in the ring layout for K == ring_kr per CTA
-    tfhe_tuning tune = {0, -1, -1, -1};   // launch shapes (0 / -1: automatic)
+    tfhe_tuning tune = {0, -1, -1, -1, -1};   // launch shapes (0 / -1: automatic)
     unsigned char* ksk_limbs = nullptr;  // int8 limbs of the key-switching key for the tensor cores
     int ks_npad = 0;                     // limb rows (4 (n+1) rounded up to the CTA tile)
 };
@@ -128,9 +128,14 @@ static void build_tables(int N, std::vector<double2>& qt, std::vector<double2>& 
 
 static std::mutex g_plan_mu;
 static std::map<std::pair<int, int>, FftPlan*> g_plans;   // (device, N)
-static std::map<int, int*> g_status;                      // device -> status word
 
-// the device status word kernels write on a bounded-wait timeout
+// The status word kernels write on a bounded-wait timeout: one static word
+// per device, so no entry point ever allocates device memory for it.  Its
+// device address is looked up once per device (the host-side name is not a
+// device address) and cached.
+static __device__ int g_device_status_word;
+static std::map<int, int*> g_status;                      // device -> address of the word
+
 int* device_status_word() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
@@ -138,10 +143,7 @@ int* device_status_word() {
     auto it = g_status.find(dev);
     if (it != g_status.end()) return it->second;
     int* w = nullptr;
-    if (cudaMalloc(&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess) {
-        cudaFree(w);
-        return nullptr;
-    }
+    if (cudaGetSymbolAddress((void**)&w, g_device_status_word) != cudaSuccess) return nullptr;
     g_status[dev] = w;
     return w;
 }
@@ -393,8 +395,9 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
         return env ? (env[0] == '1' ? 1 : 0) : 0;
     }();
     args.prefetch = (tune && tune->prefetch >= 0) ? tune->prefetch : prefetch_env;
+    args.l2_prefetch = (tune && tune->l2_prefetch == 0) ? 0 : 1;
     args.status = status ? status : device_status_word();
-    if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word allocation failed");
+    if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
     int per_sm = 1;
     TFHE_TRY(prepare_kernel((const void*)kern, sh.nt, sh.smem, &per_sm));
     // persistent CTAs: as many as fit on the SMs, looping over ciphertext
@@ -540,8 +543,10 @@ static int launch_ks(const tfhe_keys* k, const uint32_t* a_in, const uint32_t* b
                      uint32_t* b_out, long long B, cudaStream_t stream) {
     // the tensor-core kernel reads the input rows with 16-byte loads
     if (k->ksk_limbs && k->tune.ks_tensor_cores != 0 && (reinterpret_cast<uintptr_t>(a_in) & 15) == 0) {
+        int* status = device_status_word();
+        if (!status) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
         KsTcArgs args{a_in, b_in, k->ksk_limbs, k->p.n_big, k->p.n, k->p.l_ks, k->p.log2_beta_ks, k->ks_npad, B,
-                      a_out, b_out, WAIT_LIMIT_CYCLES, device_status_word(), 0, 0, nullptr};
+                      a_out, b_out, WAIT_LIMIT_CYCLES, status, 0, 0, nullptr};
         return launch_ks_tc(args, stream);
     }
     const long long ldk = k->ldk, l = k->p.l_ks;
@@ -1120,12 +1125,13 @@ int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* 
 int tfhe_keys_set_tuning(tfhe_keys* keys, const tfhe_tuning* tuning) {
     if (!keys) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys is NULL");
     if (!tuning) {
-        keys->tune = tfhe_tuning{0, -1, -1, -1};
+        keys->tune = tfhe_tuning{0, -1, -1, -1, -1};
         return TFHE_OK;
     }
     if (tuning->ciphertexts_per_cta < 0 || tuning->ciphertexts_per_cta > 64 || tuning->prefetch < -1 ||
         tuning->prefetch > 1 || tuning->persistent < -1 || tuning->persistent > 1 ||
-        tuning->ks_tensor_cores < -1 || tuning->ks_tensor_cores > 1)
+        tuning->ks_tensor_cores < -1 || tuning->ks_tensor_cores > 1 || tuning->l2_prefetch < -1 ||
+        tuning->l2_prefetch > 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "tuning out of range");
     keys->tune = *tuning;
     return TFHE_OK;
@@ -1213,12 +1219,12 @@ int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int3
 // an XLA custom call whose runtime has preallocated most of the GPU, a
 // serving loop that forbids allocation on its latency path, or code running
 // under an external memory manager.  Every GPU that loads the library holds
-// this array until the process exits.  Word 0 of the header is the status
-// word of the call (bounded-wait timeouts of the key-ring kernel).
+// this array until the process exits.  Bounded-wait timeouts of both kernels
+// of the call go to the device status word (itself a static device
+// variable), read with tfhe_device_status like those of every other entry.
 // ---------------------------------------------------------------------------
-constexpr size_t NOALLOC_HEADER_WORDS = 64;                       // 256 bytes
 constexpr size_t NOALLOC_SCRATCH_WORDS = (size_t(8) << 20) / 4;   // 8 MiB of key-switched LWEs
-static __device__ __align__(256) uint32_t g_pbs_noalloc_scratch[NOALLOC_HEADER_WORDS + NOALLOC_SCRATCH_WORDS];
+static __device__ __align__(256) uint32_t g_pbs_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
 
 static std::mutex g_noalloc_mu;
 static std::map<int, uint32_t*> g_noalloc_base;   // device -> address of the array
@@ -1255,14 +1261,11 @@ int tfhe_pbs_noalloc(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t
                         std::to_string(NOALLOC_SCRATCH_WORDS * 4) + " bytes (at most " + std::to_string(max_batch) +
                         " ciphertexts for n = " + std::to_string(n) + "); split the batch or use tfhe_pbs");
     cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
-    uint32_t* base = nullptr;
-    TFHE_TRY(noalloc_base(&base));
-    int* status = reinterpret_cast<int*>(base);
-    uint32_t* ks = base + NOALLOC_HEADER_WORDS;
+    uint32_t* ks = nullptr;
+    TFHE_TRY(noalloc_base(&ks));
     uint32_t* ks_b = ks + (size_t)batch * n;
-    TFHE_TRY(check_cuda(cudaMemsetAsync(status, 0, sizeof(int), stream), "clear status word"));
     TFHE_TRY(launch_ks(keys, a_in, b_in, ks, ks_b, batch, stream));
-    return br_native(keys, ks, ks_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch, stream, status);
+    return br_native(keys, ks, ks_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch, stream, nullptr);
 }
 
 }  // extern "C"

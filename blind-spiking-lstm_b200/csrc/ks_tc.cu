@@ -20,6 +20,9 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "tfhe_b200.h"
 #include "tfhe_dispatch.h"
@@ -221,12 +224,28 @@ size_t ks_tc_smem_bytes(int l) { return (size_t)2 * (KTC_M + KTC_N) * 2 * l * 16
 
 int ks_tc_columns() { return KTC_N; }
 
+// the dynamic shared-memory attribute is set once per kernel and device, so
+// later launches make no attribute calls (and can be captured in a graph)
+static std::mutex g_tc_attr_mu;
+static std::set<std::pair<int, const void*>> g_tc_attr_done;
+
+static int tc_set_smem_once(const void* kern, size_t smem) {
+    int dev = 0;
+    const cudaError_t ge = cudaGetDevice(&dev);
+    if (ge != cudaSuccess) return check_cuda(ge, "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(g_tc_attr_mu);
+    if (g_tc_attr_done.count({dev, kern})) return TFHE_OK;
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "tensor-core contraction attribute");
+    g_tc_attr_done.insert({dev, kern});
+    return TFHE_OK;
+}
+
 template <int L, bool PACK>
 static int launch_l(const KsTcArgs& args, cudaStream_t stream) {
     const size_t smem = ks_tc_smem_bytes(L);
-    const cudaError_t e =
-        cudaFuncSetAttribute(ks_tc_kernel<L, PACK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "tensor-core contraction attribute");
+    const int rc = tc_set_smem_once((const void*)ks_tc_kernel<L, PACK>, smem);
+    if (rc != TFHE_OK) return rc;
     const dim3 grid((unsigned)(args.npad / KTC_N), (unsigned)((args.B + KTC_M - 1) / KTC_M));
     count_launch();
     ks_tc_kernel<L, PACK><<<grid, KTC_THREADS, smem, stream>>>(args);

@@ -8,8 +8,15 @@ do not fit the array must be refused with a clear error.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test; it also passes on its own in a fresh process.
+One test runs the entry point as the very first bootstrap of a fresh process
+(no tfhe_pbs before it) and checks that the device's free memory and the
+stream-ordered pool's usage do not move across the call.
 """
 import ctypes
+import json
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -80,3 +87,79 @@ def test_noalloc_refuses_batches_beyond_the_static_array():
     assert rc == 1
     assert b"exceeds the static scratch" in _lib.load().tfhe_last_error()
     eng.close()
+
+
+# Runs in a fresh interpreter: key upload and every buffer first, then the
+# no-allocation bootstrap as the process's first bootstrap of any kind.
+# Modules load eagerly, so a lazily loaded kernel image cannot be mistaken
+# for an allocation by the call.
+_FRESH_PROCESS = r"""
+import ctypes, json, sys
+import numpy as np
+import torch
+from cuda.bindings import runtime as rt
+sys.path[:0] = [TESTS, ROOT, PKG]
+from pbs_cases import PARAMS, inputs, keys, step_body
+from tfhe_b200 import _lib
+from tfhe_b200.engine import Keys, _ptr, _stream, device_u32
+from tfhe_b200.params import ParamSet
+
+name, batch, n_lut = "tiny_c3", 37, 2
+p, k = PARAMS[name], keys(name)
+lg = lambda v: int(round(np.log2(v)))
+ps = ParamSet(name, N=p["N"], n=p["n"], log2_beta_bs=lg(p["beta_bs"]), l_bs=p["l_bs"],
+              collapse=p["collapse"], log2_beta_ks=lg(p["beta_ks"]), l_ks=p["l_ks"],
+              sigma_glwe=p["sigma_glwe"], sigma_lwe=p["sigma_lwe"])
+eng = Keys.create(ps, k.bsk_coeff, k.ksk[0], k.ksk[1].reshape(k.ksk[1].shape[:2]))
+lib = _lib.load()
+msgs, a, b = inputs(name, batch, seed_offset=300)
+a_d, b_d = device_u32(a), device_u32(b.reshape(-1))
+lut = device_u32(np.stack([np.zeros(p["N"]), step_body(name)])[None])
+outs = [(torch.full((batch, n_lut, p["N"]), -1, dtype=torch.int32, device="cuda"),
+         torch.full((batch, n_lut), -1, dtype=torch.int32, device="cuda")) for _ in range(2)]
+torch.cuda.synchronize()
+
+def pool_used_high():
+    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, v = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh)
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(v)
+
+before = (torch.cuda.mem_get_info()[0], pool_used_high(), torch.cuda.memory_reserved())
+rcs = []
+for oa, ob in outs:
+    rcs.append(lib.tfhe_pbs_noalloc(eng.handle, _ptr(a_d), _ptr(b_d), _ptr(lut), 1, n_lut,
+                                    _ptr(oa), _ptr(ob), batch, _stream()))
+torch.cuda.synchronize()
+after = (torch.cuda.mem_get_info()[0], pool_used_high(), torch.cuda.memory_reserved())
+v = ctypes.c_int32(-1)
+lib.tfhe_device_status(ctypes.byref(v), 0)
+want_a, want_b = eng.pbs(a_d, b_d, lut, n_lut=n_lut)
+torch.cuda.synchronize()
+same = all(torch.equal(oa, want_a) and torch.equal(ob, want_b) for oa, ob in outs)
+print("RESULT " + json.dumps({"rcs": rcs, "before": before, "after": after, "status": v.value,
+                              "same": same}))
+"""
+
+
+def test_noalloc_first_call_in_fresh_process_allocates_nothing():
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    code = (f"TESTS, ROOT, PKG = {here!r}, {root!r}, {os.path.join(root, 'blind-spiking-lstm_b200')!r}\n"
+            + _FRESH_PROCESS)
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    proc = subprocess.run([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE,
+                          stderr=subprocess.STDOUT, text=True, timeout=600)
+    assert proc.returncode == 0, proc.stdout[-4000:]
+    line = next(ln for ln in proc.stdout.splitlines() if ln.startswith("RESULT "))
+    res = json.loads(line[len("RESULT "):])
+    assert res["rcs"] == [0, 0]
+    free0, pool0, torch0 = res["before"]
+    free1, pool1, torch1 = res["after"]
+    assert free1 == free0, f"free device memory moved across the calls: {free0} -> {free1}"
+    assert pool1 == pool0, f"the stream-ordered pool was used: high-water {pool0} -> {pool1}"
+    assert torch1 == torch0
+    assert res["status"] == 0, "a bounded wait timed out"
+    # and the results are tfhe_pbs's, bit for bit, on both calls
+    assert res["same"]
