@@ -24,6 +24,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -51,6 +52,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-per-core", type=int, default=8,
                     help="ciphertexts per host core in each step of the reference arm")
+    ap.add_argument("--no-lstm", action="store_true",
+                    help="leave the encrypted Spike-LSTM keys out of the default (PBS) line")
     ap.add_argument("--lstm", action="store_true",
                     help="one encrypted Spike-LSTM layer + head: sequences/s (one GPU)")
     ap.add_argument("--seq-len", type=int, default=32)
@@ -63,6 +66,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=2.0, help="requests per second (--serve)")
     ap.add_argument("--requests", type=int, default=48, help="requests per serving run (--serve)")
     ap.add_argument("--max-slots", type=int, default=64)
+    ap.add_argument("--clocks-log", default=None,
+                    help="file for the nvidia-smi clock samples of the timed region (default: a temporary file)")
     ap.add_argument("--sweep", default=None,
                     help="comma-separated batch sizes: print one line per batch comparing the plain launch with "
                          "the persistent, autotuned, CUDA-graph launch (one GPU)")
@@ -106,11 +111,11 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, path=None):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv") \
-            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/tfhe_clocks_{os.getpid()}.csv"
+        # the samples go to the caller's file (--clocks-log) or a temporary one
+        self.path = path or os.path.join(tempfile.gettempdir(), f"tfhe_clocks_{os.getpid()}_{gpu_index}.csv")
 
     def start(self):
         try:
@@ -192,7 +197,7 @@ def run_engine(args, rank, world, local_rank, dist):
     torch.cuda.synchronize()
     peak_fp64 = probe_fp64_peak()
 
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(local_rank, args.clocks_log)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks.start()
@@ -250,6 +255,10 @@ def run_engine(args, rank, world, local_rank, dist):
     eng.close()
     if rank != 0:
         return None
+    lstm = None
+    if world == 1 and not args.no_lstm:
+        torch.cuda.empty_cache()
+        lstm = lstm_summary(args, dev)
 
     total = B * args.steps * world
     value = total / (dev_ms * 1e-3)
@@ -284,7 +293,81 @@ def run_engine(args, rank, world, local_rank, dist):
         "gpu_launches": gpu_launches,
         "clocks": clk,
     }
+    if lstm is not None:
+        line["lstm"] = lstm
     return line
+
+
+def lstm_summary(args, dev, steps=2, warmup=1):
+    """The one-layer encrypted Spike-LSTM workload (16 sequences of 32
+    Zipf(1.1) tokens over 8192, embedding 64, hidden 128, 4 packed LUTs,
+    weights in [-7, 7], head) timed as extra keys of the PBS line: seq/s on
+    device-resident inputs, end to end with the inputs copied from pinned
+    host memory and the logits copied back inside the timed region, and the
+    plain FP64 per-gate form (one bootstrap launch per gate and sequence, one
+    ciphertext per CTA, no persistence or key prefetch, key switch on CUDA
+    cores) on the same model and inputs."""
+    import numpy as np
+    import torch
+    from tfhe_b200 import spike_model as SM
+
+    cfg = SM.SpikeModelConfig()
+    model = SM.build_model(cfg, args.seed)
+    dm = SM.to_device(model, dev)
+    rng = np.random.default_rng(args.seed + 5)
+    S, T = 16, 32
+    tokens = SM.sample_tokens(rng, S, T, cfg.vocab, cfg.zipf)
+    xs_h = torch.from_numpy(SM.encrypt_tokens(model, tokens, rng).view(np.int32)).pin_memory()
+    xs_d = xs_h.to(dev)
+    stream = torch.cuda.current_stream()
+    pbs = dm.keys.pbs
+
+    def forward(xs, per_gate=False):
+        H, _ = SM.run_layers(dm, xs, per_gate=per_gate)
+        return dm.head(H)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, out
+
+    dev_ms, (la, lb) = timed(lambda: forward(xs_d))
+    la_h = torch.empty(la.shape, dtype=torch.int32).pin_memory()
+    lb_h = torch.empty(lb.shape, dtype=torch.int32).pin_memory()
+    xs_e = torch.empty_like(xs_d)
+
+    def e2e():
+        xs_e.copy_(xs_h, non_blocking=True)
+        a, b = forward(xs_e)
+        la_h.copy_(a, non_blocking=True)
+        lb_h.copy_(b, non_blocking=True)
+        return a, b
+
+    e2e_ms, _ = timed(e2e)
+    pbs.set_tuning(1, 0, 0, 0, 0)
+    gate_ms, (ga, gb) = timed(lambda: forward(xs_d, per_gate=True))
+    pbs.set_tuning()
+    same = bool(torch.equal(ga, la) and torch.equal(gb, lb))
+    logits = SM.decrypt_logits(model, la_h, lb_h)
+    plain, _ = SM.plain_forward(model, tokens)
+    return {"workload": f"one-layer encrypted Spike-LSTM: {S} sequences x {T} Zipf(1.1) tokens over {cfg.vocab}, "
+                        f"embedding {cfg.emb_dim}, hidden {cfg.hidden}, {cfg.n_lut} packed LUTs, weights [-7, 7], "
+                        f"head; PBS {cfg.pbs.name}; torus q = 2^32",
+            "seq_per_s": round(S / dev_ms * 1e3, 3), "ms_per_batch": round(dev_ms, 2),
+            "e2e_seq_per_s": round(S / e2e_ms * 1e3, 3),
+            "e2e_bytes": {"h2d": int(xs_h.numel() * 4), "d2h": int((la_h.numel() + lb_h.numel()) * 4)},
+            "plain_fp64_per_gate_seq_per_s": round(S / gate_ms * 1e3, 3),
+            "speedup_vs_plain_per_gate": round(gate_ms / dev_ms, 3),
+            "outputs_equal_per_gate": same,
+            "logit_sign_agreement_vs_plaintext": float(np.mean(np.sign(logits) == np.sign(plain))),
+            "steps": steps, "warmup": warmup}
 
 
 def run_lstm(args):
@@ -328,7 +411,7 @@ def run_lstm(args):
     for _ in range(args.warmup):
         forward(xs_d)
     torch.cuda.synchronize()
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(0, args.clocks_log)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n_launch0 = launch_count()
@@ -424,7 +507,7 @@ def run_serve(args):
     torch.cuda.synchronize()
 
     reqs = make_requests(args.requests, args.rate)
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(0, args.clocks_log)
     clocks.start()
     srv = SpikeLstmServer(sm, slots, t_max, dev)
     done = run_arrivals(srv, reqs)
@@ -463,11 +546,13 @@ def run_serve(args):
 
 
 def run_sweep(args, batches):
-    """Batch sweep at the 2048 parameter set: for every batch size, the plain
-    launch (one CTA wave after another, automatic shape, direct calls) and
-    the persistent, autotuned launch replayed from a CUDA graph.  Both arms
-    time key switch + blind rotation + extraction on device-resident inputs
-    with CUDA events and decrypt every output."""
+    """Batch sweep at the 2048 parameter set: for every batch size, three
+    arms on the same inputs: the plain FP64 per-gate form (one ciphertext per
+    CTA, grid = batch, no persistence or key prefetch, key switch on CUDA
+    cores), the automatic shape on a non-persistent grid (direct calls), and
+    the persistent, autotuned launch replayed from a CUDA graph.  Every arm
+    times key switch + blind rotation + extraction on device-resident inputs
+    with CUDA events and decrypts every output."""
     import numpy as np
     import torch
     from tfhe_b200 import client
@@ -509,13 +594,21 @@ def run_sweep(args, batches):
                                  keys.sk_glwe, T_OUT)
             return int(np.sum(dec != expect[:B]))
 
-        eng.set_tuning(0, -1, 0)
-
-        def plain():
+        def direct():
             eng.keyswitch(a_d[:B], b_d[:B], ka, kb)
             eng.cuboot_merge(ka, kb, lut_d[:B], 1, oa, ob)
 
-        plain_ms = timed(plain)
+        # the plain FP64 form: one ciphertext per CTA and one CTA per
+        # ciphertext (grid = batch, as the reference's mul_bootstrap kernel
+        # launches), no persistence, no key prefetch into L2 or L1, key switch
+        # on CUDA cores
+        eng.set_tuning(1, 0, 0, 0, 0)
+        gate_ms = timed(direct)
+        gate_err = errors(oa, ob)
+        gate_a, gate_b = oa.clone(), ob.clone()
+        # the engine's automatic shape on a non-persistent grid
+        eng.set_tuning(0, -1, 0)
+        plain_ms = timed(direct)
         plain_err = errors(oa, ob)
         plain_shape = eng.launch_shape(B)
 
@@ -526,11 +619,15 @@ def run_sweep(args, batches):
         graph.b.copy_(b_d[:B])
         tuned_ms = timed(graph.graph.replay)
         tuned_err = errors(graph.out_a, graph.out_b)
-        same = bool(torch.equal(graph.out_a, oa) and torch.equal(graph.out_b, ob))
+        same = bool(torch.equal(graph.out_a, oa) and torch.equal(graph.out_b, ob) and torch.equal(gate_a, oa)
+                    and torch.equal(gate_b, ob))
         del graph
         eng.set_tuning()
         out.append({"sweep": f"PBS+KS n={p.n} N={p.N} gadget 2^{p.log2_beta_bs}x{p.l_bs} KS 2^{p.log2_beta_ks}x{p.l_ks} "
                               f"c={p.collapse}", "batch": B, "steps": steps,
+                    "plain_fp64_per_gate": {"ms_per_batch": round(gate_ms, 4), "PBS/s": round(B / gate_ms * 1e3, 1),
+                                            "decrypt_errors": gate_err, "K": 1, "grid": B, "persistent": 0,
+                                            "key_prefetch": "off", "key_switch": "CUDA cores"},
                     "plain": {"ms_per_batch": round(plain_ms, 4), "PBS/s": round(B / plain_ms * 1e3, 1),
                               "decrypt_errors": plain_err, "K": plain_shape[0], "persistent": 0},
                     "persistent_autotuned_graph": {"ms_per_batch": round(tuned_ms, 4),
@@ -538,7 +635,8 @@ def run_sweep(args, batches):
                                                    "decrypt_errors": tuned_err,
                                                    "shape": {"K": shape[0], "prefetch": shape[1],
                                                              "persistent": shape[2]}},
-                    "outputs_equal": same, "speedup": round(plain_ms / tuned_ms, 3)})
+                    "outputs_equal": same, "speedup": round(plain_ms / tuned_ms, 3),
+                    "speedup_vs_per_gate": round(gate_ms / tuned_ms, 3)})
     eng.close()
     return out
 

@@ -58,6 +58,7 @@ struct BrArgs {
     // key ring (KR > 0): stages of the shared-memory ring, wait bound
     int ring_stages;
     int prefetch;             // L1 prefetch of the next pattern's key words: 1 on, 0 off, -1 by path
+    int l2_prefetch;          // 1: bring the next group's key block into L2 during each group
     long long wait_limit;     // clock cycles per mbarrier wait
     int* status;              // device status word (tfhe_device_status)
 };
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
         if constexpr (KR == 0 && !REFLAYOUT) {
             // the next group's key block (all CTAs together: each its share)
             // into L2 while this group runs
-            if (tid == 0 && g + 1 < args.G) {
+            if (tid == 0 && g + 1 < args.G && args.l2_prefetch) {
                 const size_t block = (size_t)2 * P * M * H * sizeof(double2);
                 const size_t share = ((block / gridDim.x) + 255) & ~(size_t)255;
                 const size_t off = (size_t)blockIdx.x * share;

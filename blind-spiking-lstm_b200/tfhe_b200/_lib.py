@@ -25,7 +25,8 @@ class TFHEError(RuntimeError):
 
 class TfheTuning(ctypes.Structure):
     _fields_ = [("ciphertexts_per_cta", ctypes.c_int32), ("prefetch", ctypes.c_int32),
-                ("persistent", ctypes.c_int32), ("ks_tensor_cores", ctypes.c_int32)]
+                ("persistent", ctypes.c_int32), ("ks_tensor_cores", ctypes.c_int32),
+                ("l2_prefetch", ctypes.c_int32)]
 
 
 class TfheParams(ctypes.Structure):

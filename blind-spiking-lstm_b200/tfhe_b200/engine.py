@@ -130,12 +130,14 @@ class Keys:
                                              _stream(stream)))
         return out_a, out_b
 
-    def set_tuning(self, ciphertexts_per_cta=0, prefetch=-1, persistent=-1, ks_tensor_cores=-1) -> None:
+    def set_tuning(self, ciphertexts_per_cta=0, prefetch=-1, persistent=-1, ks_tensor_cores=-1,
+                   l2_prefetch=-1) -> None:
         """Launch shapes of this key set (speed only; 0 / -1 mean automatic):
-        the blind rotation's ciphertexts per CTA, L1 prefetch and persistent
-        CTAs, and whether the key switch runs on the tensor cores.
-        tfhe_keys_set_tuning."""
-        t = _lib.TfheTuning(int(ciphertexts_per_cta), int(prefetch), int(persistent), int(ks_tensor_cores))
+        the blind rotation's ciphertexts per CTA, L1 prefetch, persistent
+        CTAs and the L2 prefetch of the next group's key block, and whether
+        the key switch runs on the tensor cores.  tfhe_keys_set_tuning."""
+        t = _lib.TfheTuning(int(ciphertexts_per_cta), int(prefetch), int(persistent), int(ks_tensor_cores),
+                            int(l2_prefetch))
         _lib.check(_lib.load().tfhe_keys_set_tuning(self.handle, ctypes.byref(t)))
         self.tuning = (int(ciphertexts_per_cta), int(prefetch), int(persistent))
 

@@ -302,9 +302,9 @@ class CipherSpikeLSTM:
         H_t = rlwe_rotate_add(H_p, self.input_dim, stream=stream)
         return H_t, C_t
 
-    def step(self, x_t, H, C, stream=None):
+    def step(self, x_t, H, C, stream=None, per_gate=False):
         """One timestep for S sequences: x_t, H, C (S, 2, N) -> (H_t, C_t)."""
-        return step_merged([(self, x_t, H, C)], stream)[0]
+        return step_merged([(self, x_t, H, C)], stream, per_gate)[0]
 
     def __call__(self, xs, stream=None):
         """xs (T, S, 2, N): the encrypted inputs of T timesteps.  Returns the
@@ -320,11 +320,13 @@ class CipherSpikeLSTM:
         return (H, C), torch.stack(hs)
 
 
-def step_merged(items, stream=None):
+def step_merged(items, stream=None, per_gate=False):
     """One timestep of several layers at once: items [(layer, x_t, H, C)]
     over any numbers of sequences.  The layers' bootstraps run as one
     launch per phase (all layers share the bootstrapping key and n_lut);
-    returns [(H_t, C_t)] in the order of items."""
+    returns [(H_t, C_t)] in the order of items.  per_gate=True instead
+    launches one bootstrap per gate of each sequence (hidden / n_lut
+    ciphertexts), the way the reference's timestep issues them."""
     gens, reqs, results = [], [], [None] * len(items)
     for i, (layer, x, H, C) in enumerate(items):
         g = layer.step_phases(x, H, C, stream)
@@ -342,7 +344,16 @@ def step_merged(items, stream=None):
             a = torch.cat([r[0] for r in reqs])
             b = torch.cat([r[1] for r in reqs])
             lut = torch.cat([r[2] for r in reqs])
-        out_a, out_b = keys.pbs(a, b, lut, n_lut, stream=stream)
+        if per_gate:
+            per = gens[0][1].per
+            N = a.shape[-1]
+            out_a = torch.empty((a.shape[0], n_lut, N), dtype=torch.int32, device=a.device)
+            out_b = torch.empty((a.shape[0], n_lut), dtype=torch.int32, device=a.device)
+            for o in range(0, a.shape[0], per):
+                keys.pbs(a[o:o + per], b[o:o + per], lut[o:o + per], n_lut, out_a[o:o + per], out_b[o:o + per],
+                         stream=stream)
+        else:
+            out_a, out_b = keys.pbs(a, b, lut, n_lut, stream=stream)
         nxt_gens, nxt_reqs, off = [], [], 0
         for (i, layer, g), c in zip(gens, counts):
             try:

@@ -132,6 +132,24 @@ def encrypt_tokens(model: SpikeModel, tokens, rng):
     return np.stack([a, b], axis=2)
 
 
+def layer_luts(cfg: SpikeModelConfig, L: PlainLayer):
+    """The layer's packed step LUTs as integer polynomials: lut_f and lut_o
+    (n_lut, hidden / n_lut, N) read the forget / output pre-activations
+    (values 0/1), lut_i (hidden / n_lut, N) the input gate, its n_lut
+    sub-LUTs weighted by eta at scale beta_x (the lut_f / lut_i / lut_o of
+    CipherSpikeLSTM, nn_tfhe/Spike_LSTM.py:73-100)."""
+    N = cfg.pbs.N
+    per = cfg.hidden // cfg.n_lut
+    lut = {g: np.stack([np.stack([plain_lut(N, cfg.n_lut, i, L.gamma[g][i, kk]) for kk in range(per)])
+                        for i in range(cfg.n_lut)]) for g in "fo"}
+    lut_i = np.zeros((per, N), dtype=np.int64)
+    for i in range(cfg.n_lut):
+        for kk in range(per):
+            lut_i[kk] += np.rint(plain_lut(N, cfg.n_lut, i, L.gamma["i"][i, kk]) * L.eta[i, kk]
+                                 * cfg.beta_x).astype(np.int64)
+    return lut["f"], lut_i, lut["o"]
+
+
 @dataclass
 class DeviceModel:
     layers: list                     # CipherSpikeLSTM per layer
@@ -157,14 +175,8 @@ def to_device(model: SpikeModel, device=None) -> DeviceModel:
             lin = Linear(per, N, 1.0, dev)
             lin.set_weights(L.W[g], L.B[g] * cfg.beta_x)
             lins.append(lin)
-        lut = {g: np.stack([np.stack([plain_lut(N, cfg.n_lut, i, L.gamma[g][i, kk]) for kk in range(per)])
-                            for i in range(cfg.n_lut)]) for g in "fo"}
-        lut_i = np.zeros((per, N), dtype=np.int64)
-        for i in range(cfg.n_lut):
-            for kk in range(per):
-                lut_i[kk] += np.rint(plain_lut(N, cfg.n_lut, i, L.gamma["i"][i, kk]) * L.eta[i, kk]
-                                     * cfg.beta_x).astype(np.int64)
-        layers.append(CipherSpikeLSTM(lk, L.in_dim, cfg.hidden, cfg.n_lut, *lins, lut["f"], lut_i, lut["o"]))
+        lut_f, lut_i, lut_o = layer_luts(cfg, L)
+        layers.append(CipherSpikeLSTM(lk, L.in_dim, cfg.hidden, cfg.n_lut, *lins, lut_f, lut_i, lut_o))
     lin1 = Linear(cfg.hidden, N, 1.0, dev)
     lin1.set_weights(model.head_W1, model.head_B1 * cfg.beta_x)
     lin2 = Linear(1, N, 1.0, dev)
@@ -173,11 +185,12 @@ def to_device(model: SpikeModel, device=None) -> DeviceModel:
     return DeviceModel(layers, CipherMLP(lk, lin1, lin2, relu), lk)
 
 
-def run_layers(dm: DeviceModel, xs, states=None, stream=None):
+def run_layers(dm: DeviceModel, xs, states=None, stream=None, per_gate=False):
     """All layers over T timesteps for S sequences: xs (T, S, 2, N).  Layer
     l + 1 reads layer l's hidden spikes moved to coefficients [0, hidden).
     Returns the final hidden RLWE of the last layer and the per-layer
-    states [(H, C)]."""
+    states [(H, C)].  per_gate=True launches one bootstrap per gate and
+    sequence (the plain per-gate form)."""
     from .lstm import rlwe_rotate_add
     T, S = xs.shape[0], xs.shape[1]
     N = xs.shape[-1]
@@ -187,7 +200,7 @@ def run_layers(dm: DeviceModel, xs, states=None, stream=None):
     for t in range(T):
         x = xs[t]
         for li, layer in enumerate(dm.layers):
-            H, C = layer.step(x, *states[li], stream)
+            H, C = layer.step(x, *states[li], stream, per_gate)
             states[li] = (H, C)
             x = rlwe_rotate_add(H, -layer.input_dim, stream=stream)
     return states[-1][0], states

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define TFHE_B200_ABI_VERSION 1
+#define TFHE_B200_ABI_VERSION 2
 
 /* status codes: the reference handler returns ffi::Error::InvalidArgument
  * for unsupported degree / l and ffi::Error::Internal for launch failures
@@ -60,6 +60,8 @@ typedef struct tfhe_tuning {
     int32_t persistent;           /* CTAs loop over ciphertext sets: -1 automatic (on), 0, 1 */
     int32_t ks_tensor_cores;      /* key switch on tcgen05 int8 tensor cores: -1 automatic (on
                                      where the parameters allow), 0 off (CUDA cores), 1 on */
+    int32_t l2_prefetch;          /* each group's key block brought into L2 during the group
+                                     before it: -1 automatic (on), 0 off, 1 on */
 } tfhe_tuning;
 
 /* library identification and the last error of the calling thread */
@@ -165,11 +167,13 @@ int tfhe_pbs(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in,
  * memory manager.  The key-switched intermediate lives in a static 8 MiB
  * device array of the library, so batch * (n + 1) * 4 bytes must fit in it
  * (at most 2822 ciphertexts for n = 742, 3323 for n = 630); larger batches
- * return TFHE_ERR_INVALID_ARGUMENT.  The array's device address is looked up
- * on the first call on each device (call once before any stream capture).
- * Every call shares the one array: calls that overlap on the GPU (other
- * streams, other threads) race and corrupt each other's results.  Same
- * arguments and results as tfhe_pbs. */
+ * return TFHE_ERR_INVALID_ARGUMENT.  The array's device address, and that of
+ * the device status word, are looked up on the first call on each device
+ * (make that first call before any stream capture).  Every call shares the
+ * one array: calls that overlap on the GPU (other streams, other threads)
+ * race and corrupt each other's results.  Bounded-wait timeouts of the call
+ * are reported by tfhe_device_status.  Same arguments and results as
+ * tfhe_pbs. */
 int tfhe_pbs_noalloc(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in,
                      const uint32_t* lut, int64_t lut_count, int32_t n_lut,
                      uint32_t* out_a, uint32_t* out_b, int64_t batch, void* stream);
@@ -196,7 +200,9 @@ int tfhe_rotate_extract_i64(const int64_t* acc, const double* b, int32_t N, int3
 
 /* Status word of the current device: kernels that wait on an mbarrier
  * give up after a bounded time and record TFHE_DEVICE_TIMEOUT here instead
- * of hanging (no counterpart in the reference).  clear != 0 resets it. */
+ * of hanging (no counterpart in the reference).  It is a static device
+ * variable of the library (no allocation), shared by every entry point,
+ * tfhe_pbs_noalloc included.  Synchronous; clear != 0 resets it. */
 #define TFHE_DEVICE_TIMEOUT 1
 int tfhe_device_status(int32_t* status_out, int32_t clear);
 
@@ -211,11 +217,6 @@ int64_t tfhe_launch_count(void);
  * TFHE_DEVICE_TIMEOUT).  Synchronous. */
 int tfhe_probe_wait_timeout(int64_t limit_cycles, int32_t* waited_out);
 
-/* Diagnostics (no counterpart in the reference): FP64 FMA throughput
- * probe for the roofline denominator.  Launches blocks x threads threads,
- * each running 8 independent FMA chains of `iters` steps; *flops receives
- * the flop count of the launch (host pointer); scratch is one device
- * double.  Time it with events on `stream`. */
 /* tfhe_pbs from HOST buffers (pinned, for overlap): the batch is processed
  * in chunks of `chunk` ciphertexts (0: automatic); each chunk's upload,
  * compute and download run on separate streams so the copies overlap the
@@ -227,6 +228,11 @@ int tfhe_pbs_host(const tfhe_keys* keys, const uint32_t* a_host, const uint32_t*
                   uint32_t* out_a_host, uint32_t* out_b_host, int64_t batch, int64_t chunk,
                   void* stream);
 
+/* Diagnostics (no counterpart in the reference): FP64 FMA throughput
+ * probe for the roofline denominator.  Launches blocks x threads threads,
+ * each running 8 independent FMA chains of `iters` steps; *flops receives
+ * the flop count of the launch (host pointer); scratch is one device
+ * double.  Time it with events on `stream`. */
 int tfhe_probe_fp64_fma(int32_t blocks, int32_t threads, int32_t iters, double* scratch,
                         double* flops, void* stream);
 

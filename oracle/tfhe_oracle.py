@@ -612,3 +612,80 @@ def step_lut(N, t_in, threshold, out_scale):
     wrap = m >= t_in
     val[wrap] = -out_scale * float(0 >= threshold)
     return val
+
+
+# --------------------------------------------------------------------------
+# the reference's own torus, q = 2^64 (parameters_crypto.py:6-32)
+# --------------------------------------------------------------------------
+# At q = 2^64 the reference holds torus values as float64 (53-bit), so its
+# arithmetic is no longer exact.  Keys and inputs are made here exactly on
+# Z/2^64 (uint64 wrapping) and then handed over as the reference's centred
+# float64 values; the float64 functions above then run unchanged at this q.
+
+REF64 = dict(q=2.0 ** 64, N=2048, n=702, beta_bs=2 ** 13, l_bs=2, collapse=3, sigma_glwe=2.0 ** 17)
+
+
+def negacyclic_mul_binary_q64(a_u64, s):
+    """a (..., N) uint64 times a binary polynomial s (N,) in Z/2^64[X]/(X^N+1),
+    exactly: a is split into four 16-bit limbs whose products with s
+    (|.| < 2^27) are exact integers, recombined with uint64 wrap-around."""
+    a = np.asarray(a_u64, dtype=np.uint64)
+    s64 = np.broadcast_to(np.asarray(s, dtype=np.int64), a.shape)
+    out = np.zeros(a.shape, dtype=np.uint64)
+    for t in range(4):
+        limb = ((a >> np.uint64(16 * t)) & np.uint64(0xFFFF)).astype(np.int64)
+        prod = negacyclic_mul_exact(limb, s64)
+        out += prod.astype(np.uint64) << np.uint64(16 * t)
+    return out
+
+
+def u64_to_centred(u):
+    """uint64 torus words -> the reference's float64 values in [-q/2, q/2]."""
+    return np.asarray(u, dtype=np.uint64).view(np.int64).astype(np.float64)
+
+
+def keygen_q64(params, seed):
+    """Collapsed bootstrapping key at q = 2^64 with the structure of
+    get_boostrapping_key_collapse (schemas/RLWE_jax.py:162-197): returns
+    (sk_glwe (N,), sk_lwe (n,), bsk_coeff (2, 2, G*M, L, N) float64 centred).
+    GLEV rows carry e * q / beta^j (left: times -s_glwe), encrypted with
+    Gaussian noise of std sigma_glwe."""
+    rng = np.random.default_rng(seed)
+    N, n, L, c = params["N"], params["n"], params["l_bs"], params["collapse"]
+    log2_beta = int(round(math.log2(params["beta_bs"])))
+    sk_glwe = rng.integers(0, 2, size=N).astype(np.int64)
+    sk_lwe = rng.integers(0, 2, size=n).astype(np.int64)
+    kron = all_binary_vectors(c)
+    eq = np.all(sk_lwe.reshape(-1, c)[:, None, :] == kron[None, :, :], axis=-1).reshape(-1).astype(np.uint64)
+    gj = np.array([1 << (64 - j * log2_beta) for j in range(1, L + 1)], dtype=np.uint64)
+    GM = eq.shape[0]
+    left = (np.uint64(0) - eq[:, None, None] * gj[None, :, None]) * sk_glwe.astype(np.uint64)[None, None, :]
+    right = np.zeros((GM, L, N), dtype=np.uint64)
+    right[:, :, 0] = eq[:, None] * gj[None, :]
+    bsk = np.empty((2, 2, GM, L, N), dtype=np.float64)
+    for side, msg in enumerate((left, right)):
+        mask = rng.integers(0, 2 ** 64, size=msg.shape, dtype=np.uint64)
+        e = np.rint(rng.standard_normal(msg.shape) * params["sigma_glwe"]).astype(np.int64).astype(np.uint64)
+        body = negacyclic_mul_binary_q64(mask, sk_glwe) + msg + e
+        bsk[side, 0], bsk[side, 1] = u64_to_centred(mask), u64_to_centred(body)
+    return sk_glwe, sk_lwe, bsk
+
+
+def encrypt_lwe_q64(messages_u64, sk, sigma, rng):
+    """LWE encryptions on Z/2^64 of uint64 messages under a binary key:
+    (a (B, n), b (B,)) as centred float64 (the reference's representation)."""
+    m = np.asarray(messages_u64, dtype=np.uint64)
+    a = rng.integers(0, 2 ** 64, size=m.shape + (len(sk),), dtype=np.uint64)
+    dot = (a * np.asarray(sk, dtype=np.uint64)).sum(axis=-1, dtype=np.uint64)
+    e = np.rint(rng.standard_normal(m.shape) * sigma).astype(np.int64).astype(np.uint64)
+    return u64_to_centred(a), u64_to_centred(dot + m + e)
+
+
+def phase_q64(a, b, sk):
+    """b - <a, s> of float64-held LWEs at q = 2^64, exactly on Z/2^64 after
+    reading the float64 values as integers: centred int64."""
+    au = np.asarray(a, dtype=np.float64)
+    bu = np.asarray(b, dtype=np.float64).reshape(au.shape[:-1])
+    to_u = lambda x: np.where(x >= 2.0 ** 63, x - 2.0 ** 64, x).astype(np.int64).astype(np.uint64)
+    dot = (to_u(au) * np.asarray(sk, dtype=np.uint64)).sum(axis=-1, dtype=np.uint64)
+    return (to_u(bu) - dot).view(np.int64)

@@ -15,11 +15,10 @@ blind rotation, many-LUT extraction) is the reference's code as written.
 Keys and inputs come from ``oracle.tfhe_oracle.keygen`` with fixed seeds
 (numpy PCG64), so only outputs are stored; the tests regenerate the keys.
 
-Run from the repository root (needs the reference checkout at
-/root/reference; the output is committed and the tests never read the
-reference):
+Run from the repository root with REFERENCE_ROOT naming a checkout of the
+reference (the output is committed and the tests never read the reference):
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -33,7 +32,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REFERENCE = os.environ.get("REFERENCE_ROOT")
+if not REFERENCE or not os.path.isdir(REFERENCE):
+    raise SystemExit("set REFERENCE_ROOT to a checkout of AMIAD-Research/Blind-Spiking-LSTM")
 
 sys.path.insert(0, os.path.join(HERE, "jaxshim"))
 sys.path.insert(0, REFERENCE)
