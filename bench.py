@@ -258,7 +258,8 @@ def run_engine(args, rank, world, local_rank, dist):
     lstm = None
     if world == 1 and not args.no_lstm:
         torch.cuda.empty_cache()
-        lstm = lstm_summary(args, dev)
+        lstm = lstm_summary(args, dev, torus_bits=64)
+        lstm_q32 = lstm_summary(args, dev, torus_bits=32)
 
     total = B * args.steps * world
     value = total / (dev_ms * 1e-3)
@@ -295,32 +296,37 @@ def run_engine(args, rank, world, local_rank, dist):
     }
     if lstm is not None:
         line["lstm"] = lstm
+        line["lstm_q32"] = lstm_q32
     return line
 
 
-def lstm_summary(args, dev, steps=2, warmup=1):
+def lstm_summary(args, dev, steps=2, warmup=1, torus_bits=64):
     """The one-layer encrypted Spike-LSTM workload (16 sequences of 32
     Zipf(1.1) tokens over 8192, embedding 64, hidden 128, 4 packed LUTs,
     weights in [-7, 7], head) timed as extra keys of the PBS line: seq/s on
     device-resident inputs, end to end with the inputs copied from pinned
     host memory and the logits copied back inside the timed region, and the
-    plain FP64 per-gate form (one bootstrap launch per gate and sequence, one
-    ciphertext per CTA, no persistence or key prefetch, key switch on CUDA
-    cores) on the same model and inputs."""
+    plain FP64 per-gate form (one bootstrap launch per gate and sequence; on
+    the 2^32 torus also one ciphertext per CTA, no persistence or key
+    prefetch, key switch on CUDA cores) on the same model and inputs.
+    torus_bits 64: the reference's own modulus and bootstrapping parameters
+    (q = 2^64, N = 2048, n = 702, gadget 2^13 x 2, collapse 3); 32: the
+    config-1 parameters on q = 2^32."""
     import numpy as np
     import torch
     from tfhe_b200 import spike_model as SM
 
-    cfg = SM.SpikeModelConfig()
+    cfg = SM.config_q64() if torus_bits == 64 else SM.SpikeModelConfig()
     model = SM.build_model(cfg, args.seed)
     dm = SM.to_device(model, dev)
     rng = np.random.default_rng(args.seed + 5)
     S, T = 16, 32
     tokens = SM.sample_tokens(rng, S, T, cfg.vocab, cfg.zipf)
-    xs_h = torch.from_numpy(SM.encrypt_tokens(model, tokens, rng).view(np.int32)).pin_memory()
+    xs_h = SM.encrypted_words(model, SM.encrypt_tokens(model, tokens, rng)).pin_memory()
     xs_d = xs_h.to(dev)
     stream = torch.cuda.current_stream()
     pbs = dm.keys.pbs
+    tunable = hasattr(pbs, "set_tuning")
 
     def forward(xs, per_gate=False):
         H, _ = SM.run_layers(dm, xs, per_gate=per_gate)
@@ -339,8 +345,8 @@ def lstm_summary(args, dev, steps=2, warmup=1):
         return e0.elapsed_time(e1) / steps, out
 
     dev_ms, (la, lb) = timed(lambda: forward(xs_d))
-    la_h = torch.empty(la.shape, dtype=torch.int32).pin_memory()
-    lb_h = torch.empty(lb.shape, dtype=torch.int32).pin_memory()
+    la_h = torch.empty(la.shape, dtype=la.dtype).pin_memory()
+    lb_h = torch.empty(lb.shape, dtype=lb.dtype).pin_memory()
     xs_e = torch.empty_like(xs_d)
 
     def e2e():
@@ -351,15 +357,17 @@ def lstm_summary(args, dev, steps=2, warmup=1):
         return a, b
 
     e2e_ms, _ = timed(e2e)
-    pbs.set_tuning(1, 0, 0, 0, 0)
+    if tunable:
+        pbs.set_tuning(1, 0, 0, 0, 0)
     gate_ms, (ga, gb) = timed(lambda: forward(xs_d, per_gate=True))
-    pbs.set_tuning()
+    if tunable:
+        pbs.set_tuning()
     same = bool(torch.equal(ga, la) and torch.equal(gb, lb))
     logits = SM.decrypt_logits(model, la_h, lb_h)
     plain, _ = SM.plain_forward(model, tokens)
     return {"workload": f"one-layer encrypted Spike-LSTM: {S} sequences x {T} Zipf(1.1) tokens over {cfg.vocab}, "
                         f"embedding {cfg.emb_dim}, hidden {cfg.hidden}, {cfg.n_lut} packed LUTs, weights [-7, 7], "
-                        f"head; PBS {cfg.pbs.name}; torus q = 2^32",
+                        f"head; PBS {cfg.pbs.name}; torus q = 2^{torus_bits}",
             "seq_per_s": round(S / dev_ms * 1e3, 3), "ms_per_batch": round(dev_ms, 2),
             "e2e_seq_per_s": round(S / e2e_ms * 1e3, 3),
             "e2e_bytes": {"h2d": int(xs_h.numel() * 4), "d2h": int((la_h.numel() + lb_h.numel()) * 4)},

@@ -75,6 +75,19 @@ SIGNATURES = {
     "tfhe_rlwe_rotate_add": (ctypes.c_int, [_P, _I32, _P, _I64, _I32, _P, _P]),
     "tfhe_u32_add": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "tfhe_rotate_extract_i64": (ctypes.c_int, [_P, _P, _I32, _I32, _I64, _P, _P, _P, _I64, _P]),
+    # the 64-bit torus (torus64.cu)
+    "tfhe64_keyswitch": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _I64, _P]),
+    "tfhe64_rotation_indices": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _I64, _P]),
+    "tfhe64_rotate_extract": (ctypes.c_int, [_P, _P, _I32, _I32, _P, _P, _I64, _P]),
+    "tfhe64_linear_extract": (ctypes.c_int, [_P, _P, _I32, _P, _I64, _I32, _P, _P, _P]),
+    "tfhe64_lut_mul_sum": (ctypes.c_int, [_P, _I32, _I32, _P, _I64, _I32, _P, _P]),
+    "tfhe64_galois_keys_create": (ctypes.c_int, [_I32, _I32, _I32, _P, _P, ctypes.POINTER(_P)]),
+    "tfhe64_galois_keys_destroy": (ctypes.c_int, [_P]),
+    "tfhe64_pack_lwe_to_rlwe": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P]),
+    "tfhe64_pack_lwes": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _I32, _I64, _P, _P]),
+    "tfhe64_rlwe_rotate_add": (ctypes.c_int, [_P, _I32, _P, _I64, _I32, _P, _P]),
+    "tfhe64_add": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "tfhe64_sample_extract": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I64, _P]),
 }
 
 _lock = threading.Lock()

@@ -11,7 +11,9 @@ encrypted-LUT preparations (pack_lwe_to_rlwe x plaintext sub-LUTs, summed
 over the n_lut packed sub-LUTs), two programmable bootstraps with n_lut
 outputs, the sum f*C + i, and two LWE -> RLWE packings.
 
-All values are uint32 torus words (q = 2^32) held in int32 tensors.
+Values are uint32 torus words (q = 2^32) held in int32 tensors, or, with
+keys of the reference's own modulus (torus64.Keys64), uint64 words (q = 2^64)
+held in int64 tensors; every operator picks its kernels by the tensors' dtype.
 """
 from __future__ import annotations
 
@@ -26,9 +28,16 @@ from .engine import Keys, _need, _ptr, _stream
 
 
 # ---------------------------------------------------------------- operators
+def _t64():
+    from . import torus64
+    return torus64
+
+
 def linear_extract(weights, bias, rlwe, out_a=None, out_b=None, stream=None):
     """Linear.__call__ for S ciphertexts: weights (J, N), bias (J) int32,
     rlwe (S, 2, N) -> (S, J, N), (S, J)."""
+    if rlwe.dtype == torch.int64:
+        return _t64().linear_extract(weights, bias, rlwe, out_a, out_b, stream)
     J, N = weights.shape
     S = rlwe.shape[0]
     _need(weights, torch.int32, (J, N), "weights")
@@ -46,6 +55,8 @@ def linear_extract(weights, bias, rlwe, out_a=None, out_b=None, stream=None):
 def lut_mul_sum(luts, rlwe, out=None, stream=None):
     """sum over g of luts[g][k] * rlwe[s][g][k]: luts (G, K, N) int32,
     rlwe (S, G, K, 2, N) -> (S, K, 2, N)."""
+    if rlwe.dtype == torch.int64:
+        return _t64().lut_mul_sum(luts, rlwe, out, stream)
     G, K, N = luts.shape
     S = rlwe.shape[0]
     _need(luts, torch.int32, (G, K, N), "luts")
@@ -153,6 +164,8 @@ class PackingKey:
 
 def rlwe_rotate_add(x, rot, y=None, out=None, stream=None):
     """X^rot * x + y for RLWEs (S, 2, N)."""
+    if x.dtype == torch.int64:
+        return _t64().rlwe_rotate_add(x, rot, y, out, stream)
     S, two, N = x.shape
     _need(x, torch.int32, (S, 2, N), "x")
     if y is not None:
@@ -165,6 +178,9 @@ def rlwe_rotate_add(x, rot, y=None, out=None, stream=None):
 
 
 def u32_add(x, y, out=None, stream=None):
+    """x + y on the torus of the tensors' dtype."""
+    if x.dtype == torch.int64:
+        return _t64().add(x, y, out, stream)
     if x.shape != y.shape:
         raise ValueError("add: shapes differ")
     _need(x, torch.int32, tuple(x.shape), "x")
@@ -208,9 +224,11 @@ class Linear:
         self.bias_np = bias.astype(np.int64)
         self.kernel_polynomial = torch.from_numpy(kern.astype(np.int64).astype(np.int32)).to(self.device)
         self.bias = torch.from_numpy(bias.astype(np.int64).astype(np.int32)).to(self.device)
+        self.bias64 = torch.from_numpy(bias.astype(np.int64)).to(self.device)
 
     def __call__(self, rlwe, stream=None):
-        return linear_extract(self.kernel_polynomial, self.bias, rlwe, stream=stream)
+        bias = self.bias64 if rlwe.dtype == torch.int64 else self.bias
+        return linear_extract(self.kernel_polynomial, bias, rlwe, stream=stream)
 
 
 @dataclass
@@ -222,6 +240,11 @@ class LayerKeys:
     pk_log2_beta: int
     pk_l: int
     packing: "PackingKey" = None   # device packing key (tensor cores where possible)
+
+    @property
+    def torus_bits(self) -> int:
+        """64 with keys of the 2^64 torus (torus64.Keys64), else 32."""
+        return 64 if self.ksp.dtype == torch.int64 else 32
 
     def pack(self, lwe_a, lwe_b, stream=None):
         if self.packing is not None:
@@ -245,10 +268,12 @@ class CipherSpikeLSTM:
         self.per = hidden_dim // n_lut
         self.W_f, self.W_i, self.W_o = linear_f, linear_i, linear_o
         dev = linear_f.device
-        i32 = lambda x: torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.int64)).astype(np.int32)).to(dev)
-        self.lut_f = i32(lut_f).reshape(n_lut, self.per, self.N)
-        self.lut_o = i32(lut_o).reshape(n_lut, self.per, self.N)
-        self.lut_i = i32(lut_i).reshape(self.per, self.N)
+        self.dtype = torch.int64 if keys.torus_bits == 64 else torch.int32
+        np_dt = np.int64 if keys.torus_bits == 64 else np.int32
+        word = lambda x: torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.int64)).astype(np_dt)).to(dev)
+        self.lut_f = word(lut_f).reshape(n_lut, self.per, self.N)
+        self.lut_o = word(lut_o).reshape(n_lut, self.per, self.N)
+        self.lut_i = word(lut_i).reshape(self.per, self.N)
         self.device = dev
 
     # prepare_LUT (nn_tfhe/activation.py:103-106) of every cell LWE, summed
@@ -271,9 +296,12 @@ class CipherSpikeLSTM:
         the bootstrap's (out_a, out_b), and returns (H_t, C_t).  Drivers can
         merge the bootstraps of several layers into one launch."""
         S, N, per, hid = x_t.shape[0], self.N, self.per, self.hidden_dim
-        c_a = torch.empty((S, hid, N), dtype=torch.int32, device=x_t.device)
-        c_b = torch.empty((S, hid), dtype=torch.int32, device=x_t.device)
-        _lib.check(_lib.load().tfhe_sample_extract(_ptr(C), N, hid, _ptr(c_a), _ptr(c_b), S, _stream(stream)))
+        if x_t.dtype == torch.int64:
+            c_a, c_b = _t64().sample_extract(C, hid, stream)
+        else:
+            c_a = torch.empty((S, hid, N), dtype=torch.int32, device=x_t.device)
+            c_b = torch.empty((S, hid), dtype=torch.int32, device=x_t.device)
+            _lib.check(_lib.load().tfhe_sample_extract(_ptr(C), N, hid, _ptr(c_a), _ptr(c_b), S, _stream(stream)))
         hx = rlwe_rotate_add(H, 0, x_t, stream=stream)
         f_a, f_b = self.W_f(hx, stream)
         i_a, i_b = self.W_i(hx, stream)
@@ -282,7 +310,7 @@ class CipherSpikeLSTM:
         # first bootstrap: [F, I] against [encrypted LUT of C, plaintext lut_i]
         in_a = torch.cat([f_a, i_a], dim=1).reshape(S * 2 * per, N)
         in_b = torch.cat([f_b, i_b], dim=1).reshape(S * 2 * per)
-        luts = torch.zeros((S, 2 * per, 2, N), dtype=torch.int32, device=x_t.device)
+        luts = torch.zeros((S, 2 * per, 2, N), dtype=x_t.dtype, device=x_t.device)
         luts[:, :per] = lut_c
         luts[:, per:, 1] = self.lut_i
         boot_a, boot_b = yield in_a, in_b, luts.reshape(S * 2 * per, 2, N)
@@ -311,7 +339,7 @@ class CipherSpikeLSTM:
         final (H, C) and the per-step H (T, S, 2, N) (jax.lax.scan of the
         reference)."""
         T, S = xs.shape[0], xs.shape[1]
-        H = torch.zeros((S, 2, self.N), dtype=torch.int32, device=xs.device)
+        H = torch.zeros((S, 2, self.N), dtype=xs.dtype, device=xs.device)
         C = torch.zeros_like(H)
         hs = []
         for t in range(T):
@@ -347,8 +375,8 @@ def step_merged(items, stream=None, per_gate=False):
         if per_gate:
             per = gens[0][1].per
             N = a.shape[-1]
-            out_a = torch.empty((a.shape[0], n_lut, N), dtype=torch.int32, device=a.device)
-            out_b = torch.empty((a.shape[0], n_lut), dtype=torch.int32, device=a.device)
+            out_a = torch.empty((a.shape[0], n_lut, N), dtype=a.dtype, device=a.device)
+            out_b = torch.empty((a.shape[0], n_lut), dtype=a.dtype, device=a.device)
             for o in range(0, a.shape[0], per):
                 keys.pbs(a[o:o + per], b[o:o + per], lut[o:o + per], n_lut, out_a[o:o + per], out_b[o:o + per],
                          stream=stream)
@@ -413,13 +441,14 @@ class CipherMLP:
     def __init__(self, keys: LayerKeys, linear1: Linear, linear2: Linear, relu_luts):
         self.keys, self.linear1, self.linear2 = keys, linear1, linear2
         dev = linear1.device
-        self.relu_luts = torch.from_numpy(np.asarray(relu_luts, dtype=np.int64).astype(np.int32)).to(dev)
+        np_dt = np.int64 if keys.torus_bits == 64 else np.int32
+        self.relu_luts = torch.from_numpy(np.asarray(relu_luts, dtype=np.int64).astype(np_dt)).to(dev)
 
     def __call__(self, H, stream=None):
         S, _, N = H.shape
         h1_a, h1_b = self.linear1(H, stream)                               # (S, J, N)
         J = h1_a.shape[1]
-        luts = torch.zeros((S, J, 2, N), dtype=torch.int32, device=H.device)
+        luts = torch.zeros((S, J, 2, N), dtype=H.dtype, device=H.device)
         luts[:, :, 1] = self.relu_luts
         y_a, y_b = self.keys.pbs.pbs(h1_a.reshape(S * J, N), h1_b.reshape(S * J), luts.reshape(S * J, 2, N), 1,
                                      stream=stream)

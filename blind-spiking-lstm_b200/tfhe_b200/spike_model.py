@@ -4,11 +4,14 @@ data, HF embeddings and trained checkpoints are not available), client key
 material, encryption of token sequences, decryption of logits, and a
 plaintext mirror of the spiking recurrence.
 
-Encoding (q = 2^32): inputs x, spikes h and cell values c sit at scale
-beta_x on the torus; a pre-activation z (integer units) is read by the
-packed step LUTs over linspace(-1, 1) at z * 4 beta_x / q
-(get_plain_LUT with s = 1, nn_tfhe/utils_spike.py:72-87); the head's ReLU
-LUT covers [0, s_head) the same way.
+Encoding: inputs x, spikes h and cell values c sit at scale beta_x on the
+torus; a pre-activation z (integer units) is read by the packed step LUTs
+over linspace(-1, 1) at z * 4 beta_x / q (get_plain_LUT with s = 1,
+nn_tfhe/utils_spike.py:72-87); the head's ReLU LUT covers [0, s_head) the
+same way.  Two tori: q = 2^32 with the config-1 bootstrapping parameters
+(beta_x = 2^22), and the reference's own q = 2^64 with its bootstrapping
+parameters (parameters_crypto.py:6-32; beta_x = 2^54, so z reads the LUTs at
+the same z / 256 on both).
 """
 from __future__ import annotations
 
@@ -18,6 +21,7 @@ import numpy as np
 import torch
 
 from . import client
+from . import client64
 from .engine import Keys
 from .lstm import CipherMLP, CipherSpikeLSTM, GaloisKeys, LayerKeys, Linear, PackingKey
 from .params import CONFIG1, ParamSet
@@ -40,10 +44,23 @@ class SpikeModelConfig:
     pk_l: int = 4
     sigma_rlwe: float = 1.0
     pbs: ParamSet = field(default_factory=lambda: CONFIG1)
+    torus_bits: int = 32
 
     @property
     def beta_x(self) -> int:
         return 1 << self.log2_beta_x
+
+
+def config_q64(**kw) -> SpikeModelConfig:
+    """The layer on the reference's torus q = 2^64 with its bootstrapping
+    parameters (N = 2048, n = 702, gadget 2^13 x 2, collapse 3, sigma 2^17),
+    Galois key 2^8 x 5 (the reference's 40 bits, 2^2 x 20), packing key
+    2^8 x 4 (the reference's, parameters_crypto.py:18-20), inputs at
+    beta_x = 2^54."""
+    base = dict(log2_beta_x=54, gal_log2_beta=8, gal_l=5, pk_log2_beta=8, pk_l=4, sigma_rlwe=2.0 ** 17,
+                pbs=client64.REF64, torus_bits=64)
+    base.update(kw)
+    return SpikeModelConfig(**base)
 
 
 def plain_lut(N, n_lut, index, gamma):
@@ -87,10 +104,11 @@ class SpikeModel:
 
 def build_model(cfg: SpikeModelConfig, seed: int = 0) -> SpikeModel:
     rng = np.random.default_rng(seed)
-    keys = client.keygen(cfg.pbs, seed + 1)
+    cl = client64 if cfg.torus_bits == 64 else client
+    keys = cl.keygen(cfg.pbs, seed + 1)
     sk = keys.sk_glwe
-    galois = client.galois_keys(sk, cfg.gal_log2_beta, cfg.gal_l, cfg.sigma_rlwe, rng)
-    ksp = client.packing_key(sk, sk, cfg.pk_log2_beta, cfg.pk_l, cfg.sigma_rlwe, rng)
+    galois = cl.galois_keys(sk, cfg.gal_log2_beta, cfg.gal_l, cfg.sigma_rlwe, rng)
+    ksp = cl.packing_key(sk, sk, cfg.pk_log2_beta, cfg.pk_l, cfg.sigma_rlwe, rng)
     per = cfg.hidden // cfg.n_lut
     layers = []
     in_dim = cfg.emb_dim
@@ -121,15 +139,23 @@ def sample_tokens(rng, count, length, vocab, a):
 
 
 def encrypt_tokens(model: SpikeModel, tokens, rng):
-    """(S, T) token ids -> (T, S, 2, N) uint32 RLWEs of the embeddings at
-    coefficients [0, emb_dim), scale beta_x."""
+    """(S, T) token ids -> (T, S, 2, N) RLWEs (uint32, or uint64 on the 2^64
+    torus) of the embeddings at coefficients [0, emb_dim), scale beta_x."""
     cfg = model.cfg
     N = cfg.pbs.N
     S, T = tokens.shape
     poly = np.zeros((T, S, N), dtype=np.int64)
     poly[..., : cfg.emb_dim] = model.embedding[tokens.T] * cfg.beta_x
-    a, b = client.encrypt_rlwe(poly, model.keys.sk_glwe, cfg.sigma_rlwe, rng)
+    cl = client64 if cfg.torus_bits == 64 else client
+    a, b = cl.encrypt_rlwe(poly, model.keys.sk_glwe, cfg.sigma_rlwe, rng)
     return np.stack([a, b], axis=2)
+
+
+def encrypted_words(model: SpikeModel, x) -> torch.Tensor:
+    """Host torus words -> the torch dtype of the model's torus (int32 /
+    int64 bit patterns), on the host."""
+    dt = np.int64 if model.cfg.torus_bits == 64 else np.int32
+    return torch.from_numpy(np.ascontiguousarray(x).view(dt))
 
 
 def layer_luts(cfg: SpikeModelConfig, L: PlainLayer):
@@ -162,11 +188,18 @@ def to_device(model: SpikeModel, device=None) -> DeviceModel:
     dev = device or torch.device("cuda", torch.cuda.current_device())
     N = cfg.pbs.N
     k = model.keys
-    pbs = Keys.create(cfg.pbs, k.bsk, k.ksk_a, k.ksk_b)
-    gk = GaloisKeys(model.galois, cfg.gal_log2_beta, cfg.gal_l, dev)
-    ksp = torch.from_numpy(np.ascontiguousarray(model.ksp).view(np.int32)).to(dev)
-    lk = LayerKeys(pbs, gk, ksp, cfg.pk_log2_beta, cfg.pk_l,
-                   PackingKey(model.ksp, cfg.pk_log2_beta, cfg.pk_l, dev))
+    if cfg.torus_bits == 64:
+        from .torus64 import GaloisKeys64, Keys64, PackingKey64
+        pbs = Keys64(k, dev)
+        gk = GaloisKeys64(model.galois, cfg.gal_log2_beta, cfg.gal_l, dev)
+        pk = PackingKey64(model.ksp, cfg.pk_log2_beta, cfg.pk_l, dev)
+        lk = LayerKeys(pbs, gk, pk.ksp, cfg.pk_log2_beta, cfg.pk_l, pk)
+    else:
+        pbs = Keys.create(cfg.pbs, k.bsk, k.ksk_a, k.ksk_b)
+        gk = GaloisKeys(model.galois, cfg.gal_log2_beta, cfg.gal_l, dev)
+        ksp = torch.from_numpy(np.ascontiguousarray(model.ksp).view(np.int32)).to(dev)
+        lk = LayerKeys(pbs, gk, ksp, cfg.pk_log2_beta, cfg.pk_l,
+                       PackingKey(model.ksp, cfg.pk_log2_beta, cfg.pk_l, dev))
     per = cfg.hidden // cfg.n_lut
     layers = []
     for L in model.layers:
@@ -195,8 +228,8 @@ def run_layers(dm: DeviceModel, xs, states=None, stream=None, per_gate=False):
     T, S = xs.shape[0], xs.shape[1]
     N = xs.shape[-1]
     if states is None:
-        states = [(torch.zeros((S, 2, N), dtype=torch.int32, device=xs.device),
-                   torch.zeros((S, 2, N), dtype=torch.int32, device=xs.device)) for _ in dm.layers]
+        states = [(torch.zeros((S, 2, N), dtype=xs.dtype, device=xs.device),
+                   torch.zeros((S, 2, N), dtype=xs.dtype, device=xs.device)) for _ in dm.layers]
     for t in range(T):
         x = xs[t]
         for li, layer in enumerate(dm.layers):
@@ -208,6 +241,10 @@ def run_layers(dm: DeviceModel, xs, states=None, stream=None, per_gate=False):
 
 def decrypt_logits(model: SpikeModel, out_a, out_b):
     """LWE logits (S, 1, N) / (S, 1) -> decrypted values in units of beta_x."""
+    if model.cfg.torus_bits == 64:
+        a = out_a.cpu().numpy().view(np.uint64).reshape(out_a.shape[0], -1)
+        b = out_b.cpu().numpy().view(np.uint64).reshape(-1)
+        return client64.phase(a, b, model.keys.sk_glwe).astype(np.float64) / model.cfg.beta_x
     a = out_a.cpu().numpy().view(np.uint32).reshape(out_a.shape[0], -1)
     b = out_b.cpu().numpy().view(np.uint32).reshape(-1)
     ph = client.phase(a, b, model.keys.sk_glwe)
@@ -221,7 +258,7 @@ def plain_forward(model: SpikeModel, tokens):
     beta_x and the final hidden spikes (S, hidden)."""
     cfg = model.cfg
     S, T = tokens.shape
-    scale = 4.0 * cfg.beta_x / 2.0 ** 32
+    scale = 4.0 * cfg.beta_x / 2.0 ** cfg.torus_bits
     per = cfg.hidden // cfg.n_lut
     sub = cfg.pbs.N // cfg.n_lut
     # the bootstrap reads sub-LUT entry rint(z * scale * sub / 2) of linspace(-1, 1, sub)

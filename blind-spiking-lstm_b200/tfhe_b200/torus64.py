@@ -1,0 +1,216 @@
+"""The engine on the reference's own torus, q = 2^64 (parameters_crypto.py:6),
+for the encrypted Spike-LSTM at the reference's parameters.  Torus values are
+uint64 bit patterns held in torch.int64 CUDA tensors; all arithmetic runs in
+libtfhe_b200.so (csrc/torus64.cu and the FP64 blind rotation of
+tfhe_mul_bootstrap at log2_q = 64).
+
+  Keys64        device bootstrapping + key-switching keys; pbs() =
+                HeavysideBoostrapper.cuboot (nn_tfhe/activation.py:148-162):
+                key switch, rotation indices, blind rotation, rotation by -b~,
+                many-LUT extraction
+  GaloisKeys64  pack_lwe_to_rlwe (schemas/text_jax.py:316-345)
+  PackingKey64  packing (schemas/text_jax.py:211-239)
+  linear_extract / lut_mul_sum / rlwe_rotate_add / add / sample_extract
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import client64 as C64
+from .engine import _need, _ptr, _stream
+
+I64 = torch.int64
+
+
+def device_u64(x, device=None) -> torch.Tensor:
+    """Host uint64 words (or integers) -> int64 CUDA tensor of the same bits."""
+    return torch.from_numpy(np.ascontiguousarray(C64.u64(x)).view(np.int64)).to(device or "cuda")
+
+
+def host_u64(t: torch.Tensor) -> np.ndarray:
+    return t.cpu().numpy().view(np.uint64)
+
+
+class Keys64:
+    """Device key material of one 64-bit parameter set."""
+
+    def __init__(self, keys: C64.ClientKeys64, device=None):
+        p = keys.params
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.params, self.device = p, dev
+        self.bsk = torch.from_numpy(C64.bsk_fourier_grouped(keys.bsk, p)).to(dev)      # (G, 2, L, 2, M, d)
+        self.rot = torch.from_numpy(C64.monomial_fourier(p.N)).to(dev)                 # (2N, d)
+        self.ksk = device_u64(keys.ksk, dev)                                            # (n_big l, n + 1)
+        self.bsk_dims = (ctypes.c_int64 * 6)(*self.bsk.shape)
+
+    def keyswitch(self, a, b, out_a=None, out_b=None, stream=None):
+        p = self.params
+        B = a.shape[0]
+        _need(a, I64, (B, p.big), "a")
+        _need(b, I64, (B,), "b")
+        out_a = out_a if out_a is not None else torch.empty((B, p.n), dtype=I64, device=a.device)
+        out_b = out_b if out_b is not None else torch.empty((B,), dtype=I64, device=a.device)
+        _lib.check(_lib.load().tfhe64_keyswitch(_ptr(self.ksk), p.big, p.n, p.l_ks, p.log2_beta_ks, _ptr(a), _ptr(b),
+                                                _ptr(out_a), _ptr(out_b), B, _stream(stream)))
+        return out_a, out_b
+
+    def blind_rotate(self, lwe_a, lut, n_lut, stream=None):
+        """The collapsed CMux chain of multiply_seq_monomial (cuTFHE/
+        multiply.py:54-92) from key-switched masks: ACC (B, 2, N) int64."""
+        p = self.params
+        B = lwe_a.shape[0]
+        _need(lwe_a, I64, (B, p.n), "lwe_a")
+        if lut.shape[0] not in (1, B):
+            raise ValueError("lut must hold 1 or B polynomial pairs")
+        _need(lut, I64, (lut.shape[0], 2, p.N), "lut")
+        idx = torch.empty((B, p.G, p.M), dtype=torch.int32, device=lwe_a.device)
+        st = _stream(stream)
+        lib = _lib.load()
+        _lib.check(lib.tfhe64_rotation_indices(_ptr(lwe_a), p.n, p.collapse, p.N, int(n_lut), _ptr(idx), B, st))
+        acc = torch.empty((B, 2, p.N), dtype=I64, device=lwe_a.device)
+        _lib.check(lib.tfhe_mul_bootstrap(st, _ptr(lut), lut.numel(), _ptr(self.bsk), self.bsk_dims, _ptr(self.rot),
+                                          self.rot.shape[0], _ptr(idx), p.log2_beta_bs, 64, p.l_bs, p.N, _ptr(acc), B))
+        return acc
+
+    def pbs(self, a, b, lut, n_lut=1, out_a=None, out_b=None, stream=None):
+        """Key switch, blind rotation, rotation by -b~ and many-LUT
+        extraction: a (B, N), b (B), lut (1|B, 2, N) -> (B, n_lut, N), (B, n_lut)."""
+        p = self.params
+        B = a.shape[0]
+        ka, kb = self.keyswitch(a, b, stream=stream)
+        acc = self.blind_rotate(ka, lut, n_lut, stream)
+        out_a = out_a if out_a is not None else torch.empty((B, n_lut, p.N), dtype=I64, device=a.device)
+        out_b = out_b if out_b is not None else torch.empty((B, n_lut), dtype=I64, device=a.device)
+        _need(out_a, I64, (B, n_lut, p.N), "out_a")
+        _need(out_b, I64, (B, n_lut), "out_b")
+        _lib.check(_lib.load().tfhe64_rotate_extract(_ptr(acc), _ptr(kb), p.N, int(n_lut), _ptr(out_a), _ptr(out_b),
+                                                     B, _stream(stream)))
+        return out_a, out_b
+
+
+class GaloisKeys64:
+    """Device Galois keys of pack_lwe_to_rlwe on Z/2^64: the Fourier
+    transforms of the four 16-bit limbs of every key polynomial."""
+
+    def __init__(self, keys_u64: np.ndarray, log2_beta: int, l: int, device=None, stream=None):
+        steps, l2, two, N = keys_u64.shape
+        if l2 != l or two != 2 or (1 << steps) != N:
+            raise ValueError("galois keys must be (log2 N, l, 2, N)")
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        src = device_u64(keys_u64, dev)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().tfhe64_galois_keys_create(N, log2_beta, l, _ptr(src), _stream(stream), ctypes.byref(h)))
+        self._h, self.N, self.log2_beta, self.l = h, N, log2_beta, l
+
+    def close(self):
+        if self._h:
+            _lib.load().tfhe64_galois_keys_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pack_lwe_to_rlwe(self, lwe_a, lwe_b, out=None, stream=None):
+        """lwe_a (R, N), lwe_b (R) -> (R, 2, N)."""
+        R = lwe_a.shape[0]
+        _need(lwe_a, I64, (R, self.N), "lwe_a")
+        _need(lwe_b, I64, (R,), "lwe_b")
+        out = out if out is not None else torch.empty((R, 2, self.N), dtype=I64, device=lwe_a.device)
+        _need(out, I64, (R, 2, self.N), "out")
+        _lib.check(_lib.load().tfhe64_pack_lwe_to_rlwe(self._h, _ptr(lwe_a), _ptr(lwe_b), R, _ptr(out),
+                                                       _stream(stream)))
+        return out
+
+
+class PackingKey64:
+    """Device packing key (n_dim, l, 2, N) on Z/2^64."""
+
+    def __init__(self, ksp_u64: np.ndarray, log2_beta: int, l: int, device=None):
+        n_dim, l2, two, N = ksp_u64.shape
+        if l2 != l or two != 2:
+            raise ValueError("packing key must be (n_dim, l, 2, N)")
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.ksp = device_u64(ksp_u64, dev)
+        self.n_dim, self.N, self.log2_beta, self.l = n_dim, N, log2_beta, l
+        self.tensor_cores = False
+
+    def pack(self, lwe_a, lwe_b, out=None, tensor_cores=-1, stream=None):
+        """lwe_a (S, T, n_dim), lwe_b (S, T) -> (S, 2, N)."""
+        S, T, nd = lwe_a.shape
+        _need(lwe_a, I64, (S, T, self.n_dim), "lwe_a")
+        _need(lwe_b, I64, (S, T), "lwe_b")
+        out = out if out is not None else torch.empty((S, 2, self.N), dtype=I64, device=lwe_a.device)
+        _need(out, I64, (S, 2, self.N), "out")
+        _lib.check(_lib.load().tfhe64_pack_lwes(_ptr(self.ksp), self.n_dim, self.N, self.log2_beta, self.l,
+                                                _ptr(lwe_a), _ptr(lwe_b), T, S, _ptr(out), _stream(stream)))
+        return out
+
+    def close(self):
+        self.ksp = None
+
+
+def linear_extract(weights, bias, rlwe, out_a=None, out_b=None, stream=None):
+    """Linear.__call__ on Z/2^64: weights (J, N) int32, bias (J) int64,
+    rlwe (S, 2, N) -> (S, J, N), (S, J)."""
+    J, N = weights.shape
+    S = rlwe.shape[0]
+    _need(weights, torch.int32, (J, N), "weights")
+    _need(bias, I64, (J,), "bias")
+    _need(rlwe, I64, (S, 2, N), "rlwe")
+    out_a = out_a if out_a is not None else torch.empty((S, J, N), dtype=I64, device=rlwe.device)
+    out_b = out_b if out_b is not None else torch.empty((S, J), dtype=I64, device=rlwe.device)
+    _lib.check(_lib.load().tfhe64_linear_extract(_ptr(weights), _ptr(bias), J, _ptr(rlwe), S, N, _ptr(out_a),
+                                                 _ptr(out_b), _stream(stream)))
+    return out_a, out_b
+
+
+def lut_mul_sum(luts, rlwe, out=None, stream=None):
+    """sum over g of luts[g][k] * rlwe[s][g][k]: luts (G, K, N) int64,
+    rlwe (S, G, K, 2, N) -> (S, K, 2, N)."""
+    G, K, N = luts.shape
+    S = rlwe.shape[0]
+    _need(luts, I64, (G, K, N), "luts")
+    _need(rlwe, I64, (S, G, K, 2, N), "rlwe")
+    out = out if out is not None else torch.empty((S, K, 2, N), dtype=I64, device=rlwe.device)
+    _lib.check(_lib.load().tfhe64_lut_mul_sum(_ptr(luts), G, K, _ptr(rlwe), S, N, _ptr(out), _stream(stream)))
+    return out
+
+
+def rlwe_rotate_add(x, rot, y=None, out=None, stream=None):
+    """X^rot * x + y for RLWEs (S, 2, N) on Z/2^64."""
+    S, two, N = x.shape
+    _need(x, I64, (S, 2, N), "x")
+    if y is not None:
+        _need(y, I64, (S, 2, N), "y")
+    out = out if out is not None else torch.empty_like(x)
+    _lib.check(_lib.load().tfhe64_rlwe_rotate_add(_ptr(x), int(rot), _ptr(y) if y is not None else None, S, N,
+                                                  _ptr(out), _stream(stream)))
+    return out
+
+
+def add(x, y, out=None, stream=None):
+    if x.shape != y.shape:
+        raise ValueError("add: shapes differ")
+    _need(x, I64, tuple(x.shape), "x")
+    _need(y, I64, tuple(y.shape), "y")
+    out = out if out is not None else torch.empty_like(x)
+    _lib.check(_lib.load().tfhe64_add(_ptr(x), _ptr(y), x.numel(), _ptr(out), _stream(stream)))
+    return out
+
+
+def sample_extract(rlwe, count, stream=None):
+    """LWEs of coefficients 0 .. count-1 of RLWEs (S, 2, N) -> (S, count, N), (S, count)."""
+    S, two, N = rlwe.shape
+    _need(rlwe, I64, (S, 2, N), "rlwe")
+    out_a = torch.empty((S, count, N), dtype=I64, device=rlwe.device)
+    out_b = torch.empty((S, count), dtype=I64, device=rlwe.device)
+    _lib.check(_lib.load().tfhe64_sample_extract(_ptr(rlwe), N, count, _ptr(out_a), _ptr(out_b), S,
+                                                 _stream(stream)))
+    return out_a, out_b

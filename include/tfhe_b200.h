@@ -311,6 +311,81 @@ int tfhe_rlwe_rotate_add(const uint32_t* x, int32_t rot, const uint32_t* y, int6
 /* out = x + y modulo 2^32 over n words (sums of LWE ciphertexts). */
 int tfhe_u32_add(const uint32_t* x, const uint32_t* y, int64_t n, uint32_t* out, void* stream);
 
+/* ------------------------------------------------------------------------
+ * The reference's own torus, q = 2^64 (parameters_crypto.py:6), where the
+ * reference holds values in float64.  Torus values are uint64 words and
+ * every integer step is exact modulo 2^64; gadget digits are the
+ * reference's decomposition (schemas/polynomial_jax.py:90-111: round half
+ * to even) evaluated exactly on the integer.  The blind rotation is
+ * tfhe_mul_bootstrap at log2_q = 64 (its FP64 chain, as the reference's).
+ * ---------------------------------------------------------------------- */
+
+/* key_switch_LWE (schemas/LWE_jax.py:97-117) on Z/2^64: ksk (n_big l_ks,
+ * n + 1) uint64, row i l_ks + j = LWE(-s_big[i] q / beta^(j+1)) as n mask
+ * words then the body; a_in (batch, n_big), b_in (batch) -> a_out
+ * (batch, n), b_out (batch).  l_ks <= 8, log2_beta_ks <= 16. */
+int tfhe64_keyswitch(const uint64_t* ksk, int32_t n_big, int32_t n, int32_t l_ks, int32_t log2_beta_ks,
+                     const uint64_t* a_in, const uint64_t* b_in, uint64_t* a_out, uint64_t* b_out,
+                     int64_t batch, void* stream);
+
+/* Rotation indices of multiply_seq_monomial (cuTFHE/multiply.py:67-79)
+ * from 64-bit masks: indices (batch, n / collapse, 2^collapse) int32,
+ * round(2N <a_g, p> / (q n_lut)) n_lut mod 2N, ready for
+ * tfhe_mul_bootstrap.  n_lut a power of two. */
+int tfhe64_rotation_indices(const uint64_t* lwe_a, int32_t n, int32_t collapse, int32_t N, int32_t n_lut,
+                            int32_t* indices, int64_t batch, void* stream);
+
+/* The steps of cuboot_merge after the chain (schemas/RLWE_jax.py:295-303)
+ * on Z/2^64: b~ = round(2N b / (q n_lut)) n_lut, ACC rotated by X^(-b~),
+ * sample_extract at 0 .. n_lut-1.  acc (batch, 2, N) int64 (the output of
+ * tfhe_mul_bootstrap at log2_q = 64), b (batch) -> out_a (batch, n_lut, N),
+ * out_b (batch, n_lut). */
+int tfhe64_rotate_extract(const int64_t* acc, const uint64_t* b, int32_t N, int32_t n_lut, uint64_t* out_a,
+                          uint64_t* out_b, int64_t batch, void* stream);
+
+/* Linear.__call__ (nn_tfhe/Spike_LSTM.py:48-58) on Z/2^64: weights (J, N)
+ * int32, bias (J) int64, rlwe (S, 2, N) -> out_a (S, J, N), out_b (S, J). */
+int tfhe64_linear_extract(const int32_t* weights, const int64_t* bias, int32_t J, const uint64_t* rlwe,
+                          int64_t S, int32_t N, uint64_t* out_a, uint64_t* out_b, void* stream);
+
+/* prepare_LUT's product summed over the packed sub-LUTs
+ * (nn_tfhe/activation.py:103-106, nn_tfhe/Spike_LSTM.py:129-132) on
+ * Z/2^64: luts (groups, per_group, N) int64, rlwe (S, groups, per_group,
+ * 2, N) -> out (S, per_group, 2, N). */
+int tfhe64_lut_mul_sum(const int64_t* luts, int32_t groups, int32_t per_group, const uint64_t* rlwe, int64_t S,
+                       int32_t N, uint64_t* out, void* stream);
+
+/* Galois keys of pack_lwe_to_rlwe (get_galois_key, schemas/RLWE_jax.py:
+ * 218-226) on Z/2^64: keys (log2 N, l, 2, N) uint64 on the device, kept as
+ * the FP64 Fourier transforms of their four 16-bit limbs so that every key
+ * product is an exact integer. */
+typedef struct tfhe64_galois_keys tfhe64_galois_keys;
+int tfhe64_galois_keys_create(int32_t N, int32_t log2_beta, int32_t l, const uint64_t* keys, void* stream,
+                              tfhe64_galois_keys** out);
+int tfhe64_galois_keys_destroy(tfhe64_galois_keys* keys);
+
+/* pack_lwe_to_rlwe (schemas/text_jax.py:316-345) on Z/2^64: lwe_a (R, N),
+ * lwe_b (R) -> out (R, 2, N). */
+int tfhe64_pack_lwe_to_rlwe(const tfhe64_galois_keys* keys, const uint64_t* lwe_a, const uint64_t* lwe_b,
+                            int64_t R, uint64_t* out, void* stream);
+
+/* packing (schemas/text_jax.py:211-239) on Z/2^64 with ksp (n_dim, l, 2, N)
+ * uint64 (get_packing_KSK, schemas/RLWE_jax.py:205-215): lwe_a
+ * (S, T, n_dim), lwe_b (S, T) -> out (S, 2, N); T <= N, l <= 8. */
+int tfhe64_pack_lwes(const uint64_t* ksp, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
+                     const uint64_t* lwe_a, const uint64_t* lwe_b, int32_t T, int64_t S, uint64_t* out,
+                     void* stream);
+
+/* out[s] = X^rot x[s] + y[s] (y may be NULL), out = x + y, and the LWEs of
+ * coefficients 0 .. count-1 of RLWEs (rotate_ciphertext, sum_ciphertext_
+ * ciphertext, sample_extract: schemas/text_jax.py:24-41, 191-208, 348-362)
+ * on Z/2^64. */
+int tfhe64_rlwe_rotate_add(const uint64_t* x, int32_t rot, const uint64_t* y, int64_t S, int32_t N,
+                           uint64_t* out, void* stream);
+int tfhe64_add(const uint64_t* x, const uint64_t* y, int64_t n, uint64_t* out, void* stream);
+int tfhe64_sample_extract(const uint64_t* rlwe, int32_t N, int32_t count, uint64_t* out_a, uint64_t* out_b,
+                          int64_t S, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -207,3 +207,50 @@ def matches(fx, key, got):
     if not np.array_equal(g.reshape(g.shape[0], -1)[0], fx[key + "_row0"]):
         return False
     return hashlib.sha256(g.tobytes()).digest() == fx[key + "_sha256"].tobytes()
+
+
+# ---------------------------------------------------------------- q = 2^64
+_Q64 = {}
+
+
+def cfg4_q64_case():
+    """The one-layer workload on the reference's own torus and bootstrapping
+    parameters (q = 2^64, N = 2048, n = 702, gadget 2^13 x 2, collapse 3),
+    one timestep of one sequence, and its head."""
+    if "case" in _Q64:
+        return _Q64["case"]
+    from tfhe_b200 import client64
+    from tfhe_b200.spike_model import build_model, config_q64, encrypt_tokens, layer_luts, sample_tokens
+    cfg = config_q64()
+    model = build_model(cfg, seed=43)
+    rng = np.random.default_rng(44)
+    tokens = sample_tokens(rng, 1, 1, cfg.vocab, cfg.zipf)
+    xs = encrypt_tokens(model, tokens, rng)                     # (1, 1, 2, N) uint64
+    L = model.layers[0]
+    lut_f, lut_i, lut_o = layer_luts(cfg, L)
+    W1, B1, W2, B2, s_head = _head(rng, cfg.emb_dim, cfg.hidden, cfg.hidden, cfg.beta_x)
+    N = cfg.pbs.N
+    hx = np.zeros(N, dtype=np.int64)
+    hx[cfg.emb_dim:cfg.emb_dim + cfg.hidden] = rng.integers(0, 2, size=cfg.hidden) * cfg.beta_x
+    ha, hb = client64.encrypt_rlwe(hx, model.keys.sk_glwe, cfg.sigma_rlwe, rng)
+    c = dict(cfg=cfg, model=model, tokens=tokens, xs=xs, lut_f=lut_f, lut_i=lut_i, lut_o=lut_o,
+             W={g: L.W[g] for g in "fio"}, B={g: L.B[g] * cfg.beta_x for g in "fio"}, gamma=L.gamma, eta=L.eta,
+             head_W1=W1, head_B1=B1, head_W2=W2, head_B2=B2, s_head=s_head, head_x=np.stack([ha, hb]),
+             hx_plain=hx)
+    _Q64["case"] = c
+    return c
+
+
+def q64_op_inputs(c):
+    """Seeded uint64 inputs of the operator fixtures at q = 2^64."""
+    rng = np.random.default_rng(203)
+    N, hid, n_lut = c["cfg"].pbs.N, c["cfg"].hidden, c["cfg"].n_lut
+    u = lambda *shape: rng.integers(0, 2 ** 64, size=shape, dtype=np.uint64)
+    return {"prep_a": u(n_lut, hid // n_lut, N), "prep_b": u(n_lut, hid // n_lut),
+            "pack_a": u(hid, N), "pack_b": u(hid)}
+
+
+def torus_dist64(x, y):
+    """|x - y| on Z/2^64 as float64 (x, y uint64 words)."""
+    d = (np.asarray(x, dtype=np.uint64) - np.asarray(y, dtype=np.uint64)).view(np.int64)
+    return np.abs(d.astype(np.float64))

@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "tfhe_b200.h")
 def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(tfhe_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(tfhe(?:64)?_[a-z0-9_]+)\s*\(", text)))
 
 
 @pytest.fixture(scope="module")
@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol(lib):
     from tfhe_b200 import _lib
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], stdout=subprocess.PIPE,
                          text=True, check=True).stdout
-    exported = set(re.findall(r"\sT\s(tfhe_\w+)", out))
+    exported = set(re.findall(r"\sT\s(tfhe(?:64)?_\w+)", out))
     missing = set(declared_functions()) - exported
     assert not missing, missing
     for name in declared_functions():
