@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--hidden", type=int, default=128)
     ap.add_argument("--layers", type=int, default=1)
     ap.add_argument("--graph", action="store_true", help="--lstm: replay each timestep from a CUDA graph")
+    ap.add_argument("--torus", type=int, choices=[32, 64], default=32,
+                    help="--lstm / --serve: the 2^32 torus (config-1 bootstrapping) or the reference's own 2^64")
     ap.add_argument("--serve", action="store_true",
                     help="continuous-batching server with Poisson arrivals: p50/p99 latency and sequences/s")
     ap.add_argument("--rate", type=float, default=2.0, help="requests per second (--serve)")
@@ -258,7 +260,7 @@ def run_engine(args, rank, world, local_rank, dist):
     lstm = None
     if world == 1 and not args.no_lstm:
         torch.cuda.empty_cache()
-        lstm = lstm_summary(args, dev, torus_bits=64)
+        lstm = lstm_summary(args, dev, steps=1, warmup=1, torus_bits=64)
         lstm_q32 = lstm_summary(args, dev, torus_bits=32)
 
     total = B * args.steps * world
@@ -393,12 +395,13 @@ def run_lstm(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
-    cfg = SM.SpikeModelConfig(hidden=args.hidden, layers=args.layers)
+    cfg = (SM.config_q64(hidden=args.hidden, layers=args.layers) if args.torus == 64
+           else SM.SpikeModelConfig(hidden=args.hidden, layers=args.layers))
     model = SM.build_model(cfg, args.seed)
     dm = SM.to_device(model, dev)
     rng = np.random.default_rng(args.seed + 5)
     tokens = SM.sample_tokens(rng, args.seqs, args.seq_len, cfg.vocab, cfg.zipf)
-    xs_h = torch.from_numpy(SM.encrypt_tokens(model, tokens, rng).view(np.int32)).pin_memory()
+    xs_h = SM.encrypted_words(model, SM.encrypt_tokens(model, tokens, rng)).pin_memory()
     xs_d = xs_h.to(dev)
     stream = torch.cuda.current_stream()
 
@@ -432,8 +435,8 @@ def run_lstm(args):
     dev_ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
 
-    la_h = torch.empty(la.shape, dtype=torch.int32).pin_memory()
-    lb_h = torch.empty(lb.shape, dtype=torch.int32).pin_memory()
+    la_h = torch.empty(la.shape, dtype=la.dtype).pin_memory()
+    lb_h = torch.empty(lb.shape, dtype=lb.dtype).pin_memory()
     xs_e = torch.empty_like(xs_d)
     e0.record(stream)
     for _ in range(args.steps):
@@ -450,7 +453,8 @@ def run_lstm(args):
     pbs_per_seq = args.seq_len * cfg.layers * 3 * (cfg.hidden // cfg.n_lut) + cfg.hidden
     return {"metric": "encrypted Spike-LSTM sequences/s (layer + head)", "value": round(args.seqs / dev_ms * 1e3, 3),
             "unit": "seq/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(dev_ms, 2), "higher_is_better": True, "dtype": "u32 torus, f64 FFT",
+            "ms_per_step": round(dev_ms, 2), "higher_is_better": True,
+            "dtype": f"u{cfg.torus_bits} torus, f64 FFT",
             "data": "synthetic: Zipf(1.1) tokens over 8192, random int weights / embeddings / thresholds",
             "config": {"workload": "Spike-LSTM", "seqs": args.seqs, "seq_len": args.seq_len, "emb_dim": cfg.emb_dim,
                        "timestep": "CUDA graph" if args.graph else "direct launches",
@@ -485,7 +489,8 @@ def run_serve(args):
     torch.cuda.set_device(0)
     hidden = args.hidden if args.hidden != 128 else 256
     layers = args.layers if args.layers != 1 else 2
-    cfg = SM.SpikeModelConfig(hidden=hidden, layers=layers)
+    cfg = (SM.config_q64(hidden=hidden, layers=layers) if args.torus == 64
+           else SM.SpikeModelConfig(hidden=hidden, layers=layers))
     model = SM.build_model(cfg, args.seed)
     dm = SM.to_device(model, dev)
     sm = DeviceStepModel(dm)
@@ -501,7 +506,7 @@ def run_serve(args):
         for i in range(n):
             T = int(rng.integers(8, 65))
             tok = SM.sample_tokens(rng, 1, T, cfg.vocab, cfg.zipf)
-            xs = torch.from_numpy(SM.encrypt_tokens(model, tok, rng).view(np.int32))[:, 0].contiguous().pin_memory()
+            xs = SM.encrypted_words(model, SM.encrypt_tokens(model, tok, rng))[:, 0].contiguous().pin_memory()
             out.append(Request(i, xs, arrival=float(arr[i])))
         return out
 
@@ -544,7 +549,7 @@ def run_serve(args):
             "data": "synthetic: Poisson arrivals, U[8,64] Zipf(1.1) tokens, random int weights",
             "config": {"workload": "Spike-LSTM serving", "rate_req_per_s": args.rate, "requests": len(done),
                        "layers": cfg.layers, "hidden": cfg.hidden, "emb_dim": cfg.emb_dim, "n_lut": cfg.n_lut,
-                       "slots": slots, "pbs": cfg.pbs.name},
+                       "slots": slots, "pbs": cfg.pbs.name, "torus": f"q = 2^{cfg.torus_bits}"},
             "latency": {k2: (round(v, 3) if isinstance(v, float) else v) for k2, v in lat.items()},
             "tokens_per_s": round(tokens / span, 2), "ticks": srv.ticks,
             "mean_batch": round(float(np.mean(srv.batch_sizes)), 2), "max_batch": int(max(srv.batch_sizes)),

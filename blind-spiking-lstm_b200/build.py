@@ -67,7 +67,8 @@ def build(force=False, jobs=None, verbose=False, extra_flags=()):
     cc = nvcc()
     jobs = jobs or min(8, os.cpu_count() or 1)
     units = [("core", os.path.join(CSRC, "core.cu"), []), ("lstm_ops", os.path.join(CSRC, "lstm_ops.cu"), []),
-             ("ks_tc", os.path.join(CSRC, "ks_tc.cu"), []), ("torus64", os.path.join(CSRC, "torus64.cu"), [])]
+             ("ks_tc", os.path.join(CSRC, "ks_tc.cu"), []), ("torus64", os.path.join(CSRC, "torus64.cu"), []),
+              ("br_fp32", os.path.join(CSRC, "br_fp32.cu"), [])]
     units += [(f"br_n{lg}", os.path.join(CSRC, "br_inst.cu"), [f"-DBR_LOGN={lg}"]) for lg in LOGNS]
     cmds = []
     objs = []

@@ -394,8 +394,10 @@ struct Trace64Args {
 //     (A_ks, B_ks) = sum_j dec_j(A') * galois_key[i][j], exact: each 16-bit
 //                    key limb's FP64 product is an integer below 2^40
 //     rlwe += (A_ks, B' + B_ks)
+constexpr int TRACE_NT = 512;     // one LWE per CTA (the CTA's shared memory holds its whole trace)
+
 template <int LOGN>
-__global__ void __launch_bounds__(256) trace64_kernel(const Trace64Args args) {
+__global__ void __launch_bounds__(TRACE_NT) trace64_kernel(const Trace64Args args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
     constexpr int LOGH = LOGN - 1;
@@ -658,7 +660,7 @@ int launch_trace(const Trace64Args& a, long long R, cudaStream_t stream) {
         cudaFuncSetAttribute(trace64_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "trace (2^64) attribute");
     count_launch();
-    trace64_kernel<LOGN><<<(unsigned)R, 256, smem, stream>>>(a);
+    trace64_kernel<LOGN><<<(unsigned)R, TRACE_NT, smem, stream>>>(a);
     return check_cuda(cudaGetLastError(), "trace (2^64) launch");
 }
 

@@ -75,6 +75,10 @@ SIGNATURES = {
     "tfhe_rlwe_rotate_add": (ctypes.c_int, [_P, _I32, _P, _I64, _I32, _P, _P]),
     "tfhe_u32_add": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "tfhe_rotate_extract_i64": (ctypes.c_int, [_P, _P, _I32, _I32, _I64, _P, _P, _P, _I64, _P]),
+    # the FP32 split-limb blind rotation (br_fp32.cu)
+    "tfhe_fp32_keys_create": (ctypes.c_int, [_P, _P, _I32, _P, ctypes.POINTER(_P)]),
+    "tfhe_fp32_keys_destroy": (None, [_P]),
+    "tfhe_fp32_cuboot_merge": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _P, _I64, _I32, _P]),
     # the 64-bit torus (torus64.cu)
     "tfhe64_keyswitch": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _I64, _P]),
     "tfhe64_rotation_indices": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _I64, _P]),

@@ -299,3 +299,56 @@ class PBSGraph:
             self.lut.copy_(lut, non_blocking=True)
         self.graph.replay()
         return self.out_a, self.out_b
+
+
+class FP32Keys:
+    """The FP32 split-limb blind rotation (tfhe_fp32_*): every FFT in FP32,
+    the bootstrapping key split into `limbs` signed limbs whose FP32 products
+    are rounded and recombined exactly modulo 2^32.  The precision ablation
+    of the external product against the FP64 engine (Keys)."""
+
+    def __init__(self, params: ParamSet, bsk_coeff, limbs: int, stream=None):
+        p = params
+        bsk = np.ascontiguousarray(to_u32(bsk_coeff).reshape(2, 2, p.G * p.M, p.l_bs, p.N))
+        cp = p.ctypes()
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().tfhe_fp32_keys_create(ctypes.byref(cp), bsk.ctypes.data, int(limbs), _stream(stream),
+                                                     ctypes.byref(out)))
+        self.params, self.limbs, self._h = p, int(limbs), out
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            _lib.load().tfhe_fp32_keys_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def cuboot_merge(self, lwe_a, lwe_b, lut, n_lut=1, out_a=None, out_b=None, ciphertexts_per_cta=0, stream=None):
+        """lwe (B, n) / (B), lut (1|B, 2, N) -> out_a (B, n_lut, N), out_b (B, n_lut)."""
+        p = self.params
+        B = lwe_a.shape[0]
+        _need(lwe_a, torch.int32, (B, p.n), "lwe_a")
+        _need(lwe_b, torch.int32, (B,), "lwe_b")
+        _need(lut, torch.int32, (lut.shape[0], 2, p.N), "lut")
+        out_a = out_a if out_a is not None else torch.empty((B, n_lut, p.N), dtype=torch.int32, device=lwe_a.device)
+        out_b = out_b if out_b is not None else torch.empty((B, n_lut), dtype=torch.int32, device=lwe_a.device)
+        _lib.check(_lib.load().tfhe_fp32_cuboot_merge(self._h, _ptr(lwe_a), _ptr(lwe_b), _ptr(lut), lut.shape[0],
+                                                      n_lut, _ptr(out_a), _ptr(out_b), None, B,
+                                                      int(ciphertexts_per_cta), _stream(stream)))
+        return out_a, out_b
+
+    def chain(self, lwe_a, lut, n_lut=1, stream=None):
+        """The accumulator after the CMux chain (B, 2, N), not rotated."""
+        p = self.params
+        B = lwe_a.shape[0]
+        _need(lwe_a, torch.int32, (B, p.n), "lwe_a")
+        _need(lut, torch.int32, (lut.shape[0], 2, p.N), "lut")
+        acc = torch.empty((B, 2, p.N), dtype=torch.int32, device=lwe_a.device)
+        b = torch.zeros((B,), dtype=torch.int32, device=lwe_a.device)
+        _lib.check(_lib.load().tfhe_fp32_cuboot_merge(self._h, _ptr(lwe_a), _ptr(b), _ptr(lut), lut.shape[0], n_lut,
+                                                      None, None, _ptr(acc), B, 0, _stream(stream)))
+        return acc

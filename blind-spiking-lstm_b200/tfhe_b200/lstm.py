@@ -404,7 +404,7 @@ class StepGraph:
         dev = layer.device
         N = layer.N
         self.layer = layer
-        self.x = torch.zeros((S, 2, N), dtype=torch.int32, device=dev)
+        self.x = torch.zeros((S, 2, N), dtype=layer.dtype, device=dev)
         self.H = torch.zeros_like(self.x)
         self.C = torch.zeros_like(self.x)
         layer.step(self.x, self.H, self.C)        # uncaptured: kernel attributes, status word, allocator

@@ -75,6 +75,7 @@ class DeviceStepModel(StepModel):
         self.dm = dm
         self.N = dm.keys.galois.N
         self.n_layers = len(dm.layers)
+        self.dtype = torch.int64 if dm.keys.torus_bits == 64 else torch.int32
 
     def state_shape(self):
         return (2, 2, self.N)
@@ -101,7 +102,8 @@ def slots_for_memory(model: StepModel, t_max: int, free_bytes: int, reserve_byte
     """Slots the pool can hold: inputs (t_max, 2, N) plus every layer's
     state per slot, within free device memory minus a reserve for the
     working buffers of one tick."""
-    per_slot = t_max * 2 * model.N * 4 + model.n_layers * int(np.prod(model.state_shape())) * 4
+    word = 8 if getattr(model, "dtype", torch.int32) == torch.int64 else 4
+    per_slot = (t_max * 2 * model.N + model.n_layers * int(np.prod(model.state_shape()))) * word
     return int(max(0, min(cap, (free_bytes - reserve_bytes) // max(per_slot, 1))))
 
 
@@ -112,8 +114,9 @@ class SpikeLstmServer:
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         self.max_slots = max_slots
         N = model.N
-        self.inputs = torch.zeros((max_slots, t_max, 2, N), dtype=torch.int32, device=self.device)
-        self.states = [torch.zeros((max_slots,) + tuple(model.state_shape()), dtype=torch.int32, device=self.device)
+        dt = getattr(model, "dtype", torch.int32)        # torus words: int32 (q = 2^32) or int64 (q = 2^64)
+        self.inputs = torch.zeros((max_slots, t_max, 2, N), dtype=dt, device=self.device)
+        self.states = [torch.zeros((max_slots,) + tuple(model.state_shape()), dtype=dt, device=self.device)
                        for _ in range(model.n_layers)]
         self.free = list(range(max_slots))
         self.live = {}                     # slot -> Request
@@ -152,7 +155,7 @@ class SpikeLstmServer:
             idx = torch.tensor(sel, dtype=torch.long, device=self.device)
             idxs.append(idx)
             if not sel:
-                xs.append(torch.zeros((0, 2, self.model.N), dtype=torch.int32, device=self.device))
+                xs.append(torch.zeros((0, 2, self.model.N), dtype=self.inputs.dtype, device=self.device))
             elif l == 0:
                 pos = torch.tensor([self.live[s].pos for s in sel], dtype=torch.long, device=self.device)
                 xs.append(self.inputs[idx, pos].contiguous())

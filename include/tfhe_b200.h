@@ -312,6 +312,31 @@ int tfhe_rlwe_rotate_add(const uint32_t* x, int32_t rot, const uint32_t* y, int6
 int tfhe_u32_add(const uint32_t* x, const uint32_t* y, int64_t n, uint32_t* out, void* stream);
 
 /* ------------------------------------------------------------------------
+ * The FP32 split-limb form of the blind rotation (the precision ablation of
+ * the external product; no counterpart in the reference, whose kernel is
+ * FP64, csrc/mul_bootstrap.cuh:20-95).  Every FFT runs in FP32 and the
+ * bootstrapping key is split into `limbs` (2..4) signed limbs of
+ * ceil(32 / limbs) bits whose FP32 products are rounded to integers and
+ * recombined exactly modulo 2^32.  bsk_coeff as for tfhe_keys_create
+ * (HOST pointer); N in {256, 1024, 2048}, l_bs <= 3 (<= 2 at N = 2048),
+ * collapse <= 3.
+ * ---------------------------------------------------------------------- */
+typedef struct tfhe_fp32_keys tfhe_fp32_keys;
+int tfhe_fp32_keys_create(const tfhe_params* params, const uint32_t* bsk_coeff, int32_t limbs, void* stream,
+                          tfhe_fp32_keys** keys_out);
+void tfhe_fp32_keys_destroy(tfhe_fp32_keys* keys);
+
+/* cuboot_merge (schemas/RLWE_jax.py:288-303) with the FP32 split-limb chain:
+ * lwe_a (batch, n), lwe_b (batch), lut (lut_count, 2, N) -> out_a
+ * (batch, n_lut, N), out_b (batch, n_lut); or, when acc_out is not NULL,
+ * the accumulator after the chain (batch, 2, N), not rotated by -b~.
+ * ciphertexts_per_cta: 1 or 2 (0: 2). */
+int tfhe_fp32_cuboot_merge(const tfhe_fp32_keys* keys, const uint32_t* lwe_a, const uint32_t* lwe_b,
+                           const uint32_t* lut, int64_t lut_count, int32_t n_lut, uint32_t* out_a,
+                           uint32_t* out_b, uint32_t* acc_out, int64_t batch, int32_t ciphertexts_per_cta,
+                           void* stream);
+
+/* ------------------------------------------------------------------------
  * The reference's own torus, q = 2^64 (parameters_crypto.py:6), where the
  * reference holds values in float64.  Torus values are uint64 words and
  * every integer step is exact modulo 2^64; gadget digits are the
