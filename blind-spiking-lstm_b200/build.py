@@ -2,8 +2,8 @@
 
     blind-spiking-lstm_b200/tfhe_b200/libtfhe_b200.so
 
-nvcc compiles core.cu and one br_inst.cu object per GLWE degree (log2 N =
-7..12) in parallel, then links them with -shared.  The build is skipped when
+nvcc compiles core.cu and one br_inst.cu and one br_inst64.cu object per
+GLWE degree (log2 N = 7..12) in parallel, then links them with -shared.  The build is skipped when
 the library is newer than every source.  Usage:
 
     python blind-spiking-lstm_b200/build.py [--force] [--jobs J]
@@ -70,6 +70,7 @@ def build(force=False, jobs=None, verbose=False, extra_flags=()):
              ("ks_tc", os.path.join(CSRC, "ks_tc.cu"), []), ("torus64", os.path.join(CSRC, "torus64.cu"), []),
               ("br_fp32", os.path.join(CSRC, "br_fp32.cu"), [])]
     units += [(f"br_n{lg}", os.path.join(CSRC, "br_inst.cu"), [f"-DBR_LOGN={lg}"]) for lg in LOGNS]
+    units += [(f"br64_n{lg}", os.path.join(CSRC, "br_inst64.cu"), [f"-DBR_LOGN={lg}"]) for lg in LOGNS]
     cmds = []
     objs = []
     for name, src, defs in units:

@@ -59,6 +59,14 @@ struct BrArgs {
     int ring_stages;
     int prefetch;             // L1 prefetch of the next pattern's key words: 1 on, 0 off, -1 by path
     int l2_prefetch;          // 1: bring the next group's key block into L2 during each group
+    // the 64-bit torus (T64 kernels, q = 2^64): the roles of lwe_a, lwe_b,
+    // lut, acc_out, out_a, out_b on uint64 words
+    const unsigned long long* lwe_a64;
+    const unsigned long long* lwe_b64;
+    const long long* lut64;
+    unsigned long long* acc_out64;
+    unsigned long long* out_a64;
+    unsigned long long* out_b64;
     long long wait_limit;     // clock cycles per mbarrier wait
     int* status;              // device status word (tfhe_device_status)
 };
@@ -112,6 +120,14 @@ __device__ __forceinline__ uint32_t ncoef(const uint32_t* p, int e) {
     return (e < N) ? v : (0u - v);
 }
 
+template <int LOGN>
+__device__ __forceinline__ unsigned long long ncoef64(const unsigned long long* p, int e) {
+    constexpr int N = 1 << LOGN;
+    e &= (2 * N - 1);
+    const unsigned long long v = p[e & (N - 1)];
+    return (e < N) ? v : (0ULL - v);
+}
+
 // inverse superstages s = S0 .. 1 (descending) over the 2K output polys
 template <int LOGH, int s>
 __device__ __forceinline__ void inverse_middle(double2* dec, int K, int P, const double2* tw, int tid, int nt) {
@@ -150,7 +166,9 @@ __device__ __forceinline__ void forward_middle(double2* dec, int npoly, const do
 // QTG: the quarter root table is read from global memory (L1-cached) instead
 // of shared memory, so two CTAs of half the ciphertexts fit on one SM.
 // XT: the CTA may have more threads than the 2 K N/16 butterfly owners.
-template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP, bool QTG = false, bool XT = false>
+// T64: the native path on the 64-bit torus (uint64 LWEs and outputs, int64
+// LUTs, q = 2^64 in the float64 chain as the reference's own arithmetic).
+template <int LOGN, int L, bool REFLAYOUT, int KR, int KTP, bool QTG = false, bool XT = false, bool T64 = false>
 __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp64_kernel(const BrArgs args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
@@ -244,6 +262,13 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             acc_lo[n2] = (double)src[on1 + Q8 * n2];
             acc_hi[n2] = (double)src[on1 + Q8 * n2 + H];
         }
+    } else if constexpr (T64) {
+        const long long* src = args.lut64 + oct * args.lut_stride + oa * N;
+#pragma unroll
+        for (int n2 = 0; n2 < 8; ++n2) {
+            acc_lo[n2] = (double)src[on1 + Q8 * n2];
+            acc_hi[n2] = (double)src[on1 + Q8 * n2 + H];
+        }
     } else {
         const uint32_t* src = args.lut + oct * args.lut_stride + oa * N;
 #pragma unroll
@@ -277,6 +302,15 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
             int r;
             if constexpr (REFLAYOUT) {
                 r = args.indices[(ct * args.G + g) * M + m];
+            } else if constexpr (T64) {
+                // rne(2N <a_g, p_m> / (q n_lut)) n_lut mod 2N on the exact group sum
+                unsigned long long v = 0ULL;
+                const unsigned long long* a = args.lwe_a64 + ct * args.lwe_n + (long long)g * args.collapse;
+                for (int c = 0; c < args.collapse; ++c)
+                    if ((m >> (args.collapse - 1 - c)) & 1) v += a[c];
+                const int ln = __ffs(args.n_lut) - 1;
+                const long long d = rne_div_pow2((long long)v, 63 - LOGN + ln);
+                r = (int)((d << ln) & (2 * N - 1));
             } else {
                 // <a_g, pattern m>, patterns in meshgrid 'ij' order
                 double v = 0.0;
@@ -599,6 +633,50 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                 dst[on1 + Q8 * n2 + H] = __double2ll_rn(acc_hi[n2]);
             }
         }
+    } else if constexpr (T64) {
+        // ACC to shared memory as uint64 words, then rotate by -b~ and
+        // extract, exactly as below on the 64-bit torus
+        typedef unsigned long long u64;
+        u64* acc = reinterpret_cast<u64*>(smem_raw);                 // [K][2][N]
+        if (owner) {
+            u64* dst = acc + (size_t)ok * 2 * N + oa * N;
+#pragma unroll
+            for (int n2 = 0; n2 < 8; ++n2) {
+                dst[on1 + Q8 * n2] = (u64)__double2ll_rn(acc_lo[n2]);
+                dst[on1 + Q8 * n2 + H] = (u64)__double2ll_rn(acc_hi[n2]);
+            }
+        }
+        for (int k = tid; k < K; k += nt) {
+            const long long ct = min(ct0 + k, args.B - 1);
+            const int ln = __ffs(args.n_lut) - 1;
+            bexp[k] = (int)((rne_div_pow2((long long)args.lwe_b64[ct], 63 - LOGN + ln) << ln) & (2 * N - 1));
+        }
+        __syncthreads();
+        const int kv = (int)min((long long)K, args.B - ct0);
+        if (args.acc_out64) {
+            for (int t = tid; t < kv * 2 * N; t += nt) {
+                const int k = t / (2 * N);
+                const int rem = t - k * 2 * N;
+                const int a = rem / N;
+                const int i = rem - a * N;
+                args.acc_out64[(ct0 + k) * 2 * N + rem] = ncoef64<LOGN>(acc + (size_t)k * 2 * N + a * N, i + bexp[k]);
+            }
+        }
+        if (args.out_a64) {
+            const int nl = args.n_lut;
+            for (int t = tid; t < kv * nl * N; t += nt) {
+                const int k = t / (nl * N);
+                const int rem = t - k * nl * N;
+                const int al = rem / N;
+                const int j = rem - al * N;
+                args.out_a64[(ct0 + k) * nl * N + rem] = ncoef64<LOGN>(acc + (size_t)k * 2 * N, al - j + bexp[k]);
+            }
+            for (int t = tid; t < kv * nl; t += nt) {
+                const int k = t / nl;
+                const int al = t - k * nl;
+                args.out_b64[(ct0 + k) * nl + al] = ncoef64<LOGN>(acc + (size_t)k * 2 * N + N, al + bexp[k]);
+            }
+        }
     } else {
         // ACC to shared memory as u32, then rotate by -b~ (RLWE_jax.py:295-297)
         // and, for the PBS, extract n_lut LWEs (RLWE_jax.py:301-303)
@@ -658,6 +736,7 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
 // ----------------------------------------------------------------------------
 struct BskConvArgs {
     const uint32_t* src;
+    const unsigned long long* src64;   // the 64-bit torus's key (then src is unused)
     double2* dst;
     const double2* qt;
     const double2* tw;
@@ -682,9 +761,16 @@ __global__ void __launch_bounds__(256) bsk_fft_kernel(const BskConvArgs a) {
     for (int idx = tid; idx < PPC * H; idx += nt) {
         const int lp = idx / H, i = idx % H;
         const long long pi = min(p0 + lp, a.npoly - 1);
-        const uint32_t* s = a.src + pi * N;
-        const double lo = (double)(int32_t)s[i];
-        const double hi = (double)(int32_t)s[i + H];
+        double lo, hi;
+        if (a.src64) {
+            const unsigned long long* s64 = a.src64 + pi * N;
+            lo = (double)(long long)s64[i];
+            hi = (double)(long long)s64[i + H];
+        } else {
+            const uint32_t* s = a.src + pi * N;
+            lo = (double)(int32_t)s[i];
+            hi = (double)(int32_t)s[i + H];
+        }
         const double2 w = a.qt[i];
         buf[lp * H + swz(i)] = make_double2(fma(w.x, lo, w.y * hi), fma(w.y, lo, -w.x * hi));
     }

@@ -371,7 +371,9 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
                               : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0, !reflayout);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
-    BrKernel kern = br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt, sh.qtg, sh.xt);
+    const bool t64 = args.lwe_a64 != nullptr;
+    BrKernel kern = t64 ? (kr == 0 ? br_fp64_t64_kernel_for(logn, L, sh.kt, sh.qtg, sh.xt) : nullptr)
+                        : br_fp64_kernel_for(logn, L, reflayout, kr, sh.kt, sh.qtg, sh.xt);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
     if (sh.K < 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT,
@@ -435,6 +437,12 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
             if (tail.out_a) tail.out_a += full * args.n_lut * N;
             if (tail.out_b) tail.out_b += full * args.n_lut;
             if (tail.out_i64) tail.out_i64 += full * 2 * N;
+            if (tail.lwe_a64) tail.lwe_a64 += full * args.lwe_n;
+            if (tail.lwe_b64) tail.lwe_b64 += full;
+            if (tail.lut64) tail.lut64 += full * args.lut_stride;
+            if (tail.acc_out64) tail.acc_out64 += full * 2 * N;
+            if (tail.out_a64) tail.out_a64 += full * args.n_lut * N;
+            if (tail.out_b64) tail.out_b64 += full * args.n_lut;
             return launch_br(tail, N, L, reflayout, 0, stream, status, tune);
         }
     }
@@ -651,18 +659,25 @@ static int validate_params(const tfhe_params* p) {
     if (p->collapse < 1 || p->collapse > 4) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported collapse (1..4)");
     if (p->n <= 0 || p->n % p->collapse) return fail(TFHE_ERR_INVALID_ARGUMENT, "n must be a positive multiple of collapse");
     if (p->n_big <= 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "n_big must be positive");
-    if (p->log2_q != 32) return fail(TFHE_ERR_INVALID_ARGUMENT, "native entry points need log2_q == 32");
-    if (p->log2_beta_bs < 1 || p->log2_beta_bs * p->l_bs > 32)
-        return fail(TFHE_ERR_INVALID_ARGUMENT, "log2_beta_bs * l_bs must be in [1, 32]");
-    if (p->l_ks < 1 || p->l_ks > KS_LMAX || p->log2_beta_ks < 1 || p->log2_beta_ks * p->l_ks > 32)
+    if (p->log2_q != 32 && p->log2_q != 64)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "native entry points need log2_q == 32 (tfhe_*) or 64 (tfhe64_*)");
+    if (p->log2_beta_bs < 1 || p->log2_beta_bs * p->l_bs > p->log2_q)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "log2_beta_bs * l_bs must be in [1, log2_q]");
+    if (p->l_ks < 1 || p->l_ks > KS_LMAX || p->log2_beta_ks < 1 || p->log2_beta_ks * p->l_ks > p->log2_q)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported key-switch base / levels");
+    if (p->log2_q == 64 && p->l_bs > 3)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "the 64-bit blind rotation supports l_bs 1..3");
     if (br_shape(p->N, p->l_bs, 1 << p->collapse, 1).K < 1)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "degree / levels do not fit in shared memory");
     return TFHE_OK;
 }
 
-static int check_keys(const tfhe_keys* k) {
+// log2_q: the torus the calling entry point works on (32: tfhe_*, 64: tfhe64_*)
+static int check_keys(const tfhe_keys* k, int log2_q = 32) {
     if (!k) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys is NULL");
+    if (k->p.log2_q != log2_q)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, log2_q == 32 ? "keys are for q = 2^64: use the tfhe64_* entry points"
+                                                            : "keys are for q = 2^32: use the tfhe_* entry points");
     int dev = -1;
     TFHE_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
     if (dev != k->device)
@@ -714,10 +729,13 @@ static int upload_ksk(tfhe_keys* k, const uint32_t* ksk_a, const uint32_t* ksk_b
     return check_cuda(cudaStreamSynchronize(stream), "ksk upload sync");
 }
 
-static int keys_common(const tfhe_params* params, tfhe_keys** out, tfhe_keys** made) {
+static int keys_common(const tfhe_params* params, tfhe_keys** out, tfhe_keys** made, int log2_q = 32) {
     if (!out) return fail(TFHE_ERR_INVALID_ARGUMENT, "keys_out is NULL");
     *out = nullptr;
     TFHE_TRY(validate_params(params));
+    if (params->log2_q != log2_q)
+        return fail(TFHE_ERR_INVALID_ARGUMENT, log2_q == 32 ? "tfhe_keys_create* need log2_q == 32"
+                                                            : "tfhe64_keys_create needs log2_q == 64");
     tfhe_keys* k = new tfhe_keys();
     k->p = *params;
     k->G = params->n / params->collapse;
@@ -731,7 +749,8 @@ static int keys_common(const tfhe_params* params, tfhe_keys** out, tfhe_keys** m
         delete k;
         return TFHE_ERR_INTERNAL;
     }
-    k->ring_kr = ring_shape(params->N, params->l_bs, k->M).kr;
+    // the key ring layout has no 64-bit kernels
+    k->ring_kr = params->log2_q == 32 ? ring_shape(params->N, params->l_bs, k->M).kr : 0;
     *made = k;
     return TFHE_OK;
 }
@@ -747,6 +766,44 @@ static void keys_free(tfhe_keys* k) {
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 static long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// The bootstrapping key (2 in, 2 out, G M, L, N) words of elem bytes (4: the
+// 32-bit torus, 8: the 64-bit one) -> the FP64 Fourier layout the blind
+// rotation reads, converted on the device.
+static int upload_bsk(tfhe_keys* k, const void* bsk_coeff, size_t elem, cudaStream_t stream) {
+    const tfhe_params& p = k->p;
+    const int N = p.N, H = N / 2, L = p.l_bs;
+    const long long npoly = 4LL * k->G * k->M * L;
+    const size_t src_bytes = (size_t)npoly * N * elem;
+    const size_t dst_bytes = (size_t)npoly * H * sizeof(double2);
+    void* d_src = nullptr;
+    int rc = check_cuda(cudaMalloc(&d_src, src_bytes), "cudaMalloc(bsk staging)");
+    if (rc == TFHE_OK) rc = check_cuda(cudaMalloc(&k->bsk, dst_bytes), "cudaMalloc(bsk)");
+    if (rc == TFHE_OK) {
+        k->bytes += (int64_t)dst_bytes;
+        rc = check_cuda(cudaMemcpyAsync(d_src, bsk_coeff, src_bytes, cudaMemcpyHostToDevice, stream), "bsk upload");
+    }
+    if (rc == TFHE_OK) {
+        BskConvArgs ca{elem == 4 ? static_cast<const uint32_t*>(d_src) : nullptr,
+                       elem == 8 ? static_cast<const unsigned long long*>(d_src) : nullptr,
+                       k->bsk, k->plan->qt, k->plan->tw, k->G, k->M, L, npoly,
+                       k->ring_kr > 0 ? k->ring_kr * H / 4 : 0};
+        const int ppc = std::max(1, 2048 / H);
+        const size_t smem = (size_t)ppc * H * sizeof(double2);
+        BrConvKernel kern = bsk_fft_kernel_for(ilog2(N));
+        rc = check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                        "cudaFuncSetAttribute(bsk fft)");
+        if (rc == TFHE_OK) {
+            count_launch();
+            kern<<<(unsigned)((npoly + ppc - 1) / ppc), 256, smem, stream>>>(ca);
+            rc = check_cuda(cudaGetLastError(), "bsk fft launch");
+        }
+        if (rc == TFHE_OK) rc = check_cuda(cudaStreamSynchronize(stream), "bsk fft");
+    }
+    cudaFree(d_src);
+    return rc;
+}
+
 
 }  // namespace tfhe
 
@@ -810,34 +867,7 @@ int tfhe_keys_create(const tfhe_params* params, const uint32_t* bsk_coeff, const
         return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL key buffer");
     }
     cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
-    const tfhe_params& p = *params;
-    const int N = p.N, H = N / 2, L = p.l_bs;
-    const long long npoly = 4LL * k->G * k->M * L;
-    const size_t src_bytes = (size_t)npoly * N * sizeof(uint32_t);
-    const size_t dst_bytes = (size_t)npoly * H * sizeof(double2);
-    uint32_t* d_src = nullptr;
-    int rc = check_cuda(cudaMalloc(&d_src, src_bytes), "cudaMalloc(bsk staging)");
-    if (rc == TFHE_OK) rc = check_cuda(cudaMalloc(&k->bsk, dst_bytes), "cudaMalloc(bsk)");
-    if (rc == TFHE_OK) {
-        k->bytes += (int64_t)dst_bytes;
-        rc = check_cuda(cudaMemcpyAsync(d_src, bsk_coeff, src_bytes, cudaMemcpyHostToDevice, stream), "bsk upload");
-    }
-    if (rc == TFHE_OK) {
-        BskConvArgs ca{d_src, k->bsk, k->plan->qt, k->plan->tw, k->G, k->M, L, npoly,
-                       k->ring_kr > 0 ? k->ring_kr * H / 4 : 0};
-        const int ppc = std::max(1, 2048 / H);
-        const size_t smem = (size_t)ppc * H * sizeof(double2);
-        BrConvKernel kern = bsk_fft_kernel_for(ilog2(N));
-        rc = check_cuda(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                        "cudaFuncSetAttribute(bsk fft)");
-        if (rc == TFHE_OK) {
-            count_launch();
-            kern<<<(unsigned)((npoly + ppc - 1) / ppc), 256, smem, stream>>>(ca);
-            rc = check_cuda(cudaGetLastError(), "bsk fft launch");
-        }
-        if (rc == TFHE_OK) rc = check_cuda(cudaStreamSynchronize(stream), "bsk fft");
-    }
-    cudaFree(d_src);
+    int rc = upload_bsk(k, bsk_coeff, sizeof(uint32_t), stream);
     if (rc == TFHE_OK) rc = upload_ksk(k, ksk_a, ksk_b, stream);
     if (rc != TFHE_OK) {
         keys_free(k);
@@ -908,6 +938,70 @@ int tfhe_keys_create_fourier(const tfhe_params* params, const double* bsk_ordere
 void tfhe_keys_destroy(tfhe_keys* keys) { keys_free(keys); }
 
 int64_t tfhe_keys_device_bytes(const tfhe_keys* keys) { return keys ? keys->bytes : 0; }
+
+// ---------------------------------------------------------------- the 64-bit torus
+int tfhe64_keys_create(const tfhe_params* params, const uint64_t* bsk_coeff, void* stream, tfhe_keys** keys_out) {
+    tfhe_keys* k = nullptr;
+    TFHE_TRY(keys_common(params, keys_out, &k, 64));
+    if (!bsk_coeff) {
+        keys_free(k);
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL key buffer");
+    }
+    const int rc = upload_bsk(k, bsk_coeff, sizeof(uint64_t), static_cast<cudaStream_t>(stream));
+    if (rc != TFHE_OK) {
+        keys_free(k);
+        return rc;
+    }
+    *keys_out = k;
+    return TFHE_OK;
+}
+
+static int br_native64(const tfhe_keys* keys, const uint64_t* lwe_a, const uint64_t* lwe_b, const int64_t* lut,
+                       int64_t lut_count, int32_t n_lut, uint64_t* acc_out, uint64_t* out_a, uint64_t* out_b,
+                       int64_t batch, cudaStream_t stream) {
+    TFHE_TRY(check_keys(keys, 64));
+    const tfhe_params& p = keys->p;
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "negative batch");
+    if (n_lut < 1 || n_lut > p.N || (n_lut & (n_lut - 1)))
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "n_lut must be a power of two in [1, N]");
+    if (lut_count != 1 && lut_count != batch) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut_count must be 1 or batch");
+    if (batch == 0) return TFHE_OK;
+    if (!lwe_a || !lwe_b || !lut || !(acc_out || (out_a && out_b)))
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    BrArgs a{};
+    a.bsk = keys->bsk;
+    a.G = keys->G;
+    a.M = keys->M;
+    a.collapse = p.collapse;
+    a.B = batch;
+    a.log2_beta = p.log2_beta_bs;
+    a.log2_q = 64;
+    a.lwe_a64 = reinterpret_cast<const unsigned long long*>(lwe_a);
+    a.lwe_b64 = reinterpret_cast<const unsigned long long*>(lwe_b);
+    a.lut64 = reinterpret_cast<const long long*>(lut);
+    a.lut_stride = lut_count == 1 ? 0 : 2LL * p.N;
+    a.n_lut = n_lut;
+    a.lwe_n = p.n;
+    a.acc_out64 = reinterpret_cast<unsigned long long*>(acc_out);
+    a.out_a64 = reinterpret_cast<unsigned long long*>(out_a);
+    a.out_b64 = reinterpret_cast<unsigned long long*>(out_b);
+    return launch_br(a, p.N, p.l_bs, false, 0, stream, nullptr, &keys->tune);
+}
+
+int tfhe64_blind_rotate(const tfhe_keys* keys, const uint64_t* lwe_a, const uint64_t* lwe_b, const int64_t* lut,
+                        int64_t lut_count, int32_t n_lut, uint64_t* acc_out, int64_t batch, void* stream) {
+    if (!acc_out && batch > 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    return br_native64(keys, lwe_a, lwe_b, lut, lut_count, n_lut, acc_out, nullptr, nullptr, batch,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int tfhe64_cuboot_merge(const tfhe_keys* keys, const uint64_t* lwe_a, const uint64_t* lwe_b, const int64_t* lut,
+                        int64_t lut_count, int32_t n_lut, uint64_t* out_a, uint64_t* out_b, int64_t batch,
+                        void* stream) {
+    if ((!out_a || !out_b) && batch > 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "NULL buffer");
+    return br_native64(keys, lwe_a, lwe_b, lut, lut_count, n_lut, nullptr, out_a, out_b, batch,
+                       static_cast<cudaStream_t>(stream));
+}
 
 int tfhe_keyswitch(const tfhe_keys* keys, const uint32_t* a_in, const uint32_t* b_in, uint32_t* a_out,
                    uint32_t* b_out, int64_t batch, void* stream) {

@@ -75,7 +75,25 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-template <int L, bool PACK>
+// gadget digit of a centred 64-bit value: rne(x / 2^sh), *rem = x - d 2^sh
+// (the reference's decomposition, schemas/polynomial_jax.py:90-111, on the
+// exact integer)
+__device__ __forceinline__ long long rne_shift64(long long x, int sh, long long* rem) {
+    long long d = x >> sh;
+    const unsigned long long low = (unsigned long long)x & ((1ULL << sh) - 1ULL);
+    const unsigned long long half = 1ULL << (sh - 1);
+    if (low > half || (low == half && (d & 1))) {
+        d += 1;
+        *rem = (long long)(low - (1ULL << sh));
+    } else {
+        *rem = (long long)low;
+    }
+    return d;
+}
+
+// W64: 64-bit torus words (q = 2^64): eight 8-bit limbs per key word, digits
+// from the exact integer, outputs recombined modulo 2^64
+template <int L, bool PACK, bool W64>
 __global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -123,7 +141,26 @@ __global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
             const long long row = row0 + r;
             const int i0 = s * KTC_COEF + half * 16;
             int8_t dig[16 * L];
-            if (row < a.B) {
+            if (W64 && row < a.B) {
+                const uint4* src = reinterpret_cast<const uint4*>(
+                    reinterpret_cast<const unsigned long long*>(a.a_in) + row * a.n_big + i0);
+#pragma unroll
+                for (int q4 = 0; q4 < 8; ++q4) {
+                    const uint4 v = src[q4];
+                    const unsigned long long w[2] = {((unsigned long long)v.y << 32) | v.x,
+                                                     ((unsigned long long)v.w << 32) | v.z};
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        long long x = (long long)w[e];
+#pragma unroll
+                        for (int j = 0; j < l; ++j) {
+                            long long rem;
+                            dig[(q4 * 2 + e) * l + j] = (int8_t)rne_shift64(x, 64 - (j + 1) * a.log2_beta, &rem);
+                            x = rem;
+                        }
+                    }
+                }
+            } else if (row < a.B) {
                 const uint4* src = reinterpret_cast<const uint4*>(a.a_in + row * a.n_big + i0);
 #pragma unroll
                 for (int q4 = 0; q4 < 4; ++q4) {
@@ -190,6 +227,31 @@ __global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
             tmem_ld8(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c, v);
             tmem_wait_ld();
             if (!ok || row >= a.B) continue;
+            if constexpr (W64) {
+                typedef unsigned long long u64;
+                const int o = (col0 + c) / 8;
+                u64 val = 0ULL;
+#pragma unroll
+                for (int t = 0; t < 8; ++t) val += (u64)(long long)(int32_t)v[t] << (8 * t);
+                if constexpr (PACK) {
+                    if (o >= 2 * a.pack_N) continue;
+                    const long long sq = row / a.pack_T;
+                    const int t = (int)(row - sq * a.pack_T);
+                    const int poly = o / a.pack_N, cc = o - poly * a.pack_N;
+                    int d = cc + t;
+                    u64 add = 0ULL - val;                  // -X^t V: negated unless it wraps past X^N
+                    if (d >= a.pack_N) {
+                        d -= a.pack_N;
+                        add = val;
+                    }
+                    atomicAdd(reinterpret_cast<u64*>(a.pack_out) + (sq * 2 + poly) * (long long)a.pack_N + d, add);
+                } else {
+                    if (o < a.n) reinterpret_cast<u64*>(a.a_out)[row * a.n + o] = val;
+                    else if (o == a.n)
+                        reinterpret_cast<u64*>(a.b_out)[row] = reinterpret_cast<const u64*>(a.b_in)[row] + val;
+                }
+                continue;
+            }
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int o = (col0 + c) / 4 + h;
@@ -241,28 +303,28 @@ static int tc_set_smem_once(const void* kern, size_t smem) {
     return TFHE_OK;
 }
 
-template <int L, bool PACK>
+template <int L, bool PACK, bool W64>
 static int launch_l(const KsTcArgs& args, cudaStream_t stream) {
     const size_t smem = ks_tc_smem_bytes(L);
-    const int rc = tc_set_smem_once((const void*)ks_tc_kernel<L, PACK>, smem);
+    const int rc = tc_set_smem_once((const void*)ks_tc_kernel<L, PACK, W64>, smem);
     if (rc != TFHE_OK) return rc;
     const dim3 grid((unsigned)(args.npad / KTC_N), (unsigned)((args.B + KTC_M - 1) / KTC_M));
     count_launch();
-    ks_tc_kernel<L, PACK><<<grid, KTC_THREADS, smem, stream>>>(args);
+    ks_tc_kernel<L, PACK, W64><<<grid, KTC_THREADS, smem, stream>>>(args);
     return check_cuda(cudaGetLastError(), "tensor-core contraction launch");
 }
 
-template <bool PACK>
+template <bool PACK, bool W64>
 static int launch_any(const KsTcArgs& args, cudaStream_t stream) {
     switch (args.l) {
-        case 1: return launch_l<1, PACK>(args, stream);
-        case 2: return launch_l<2, PACK>(args, stream);
-        case 3: return launch_l<3, PACK>(args, stream);
-        case 4: return launch_l<4, PACK>(args, stream);
-        case 5: return launch_l<5, PACK>(args, stream);
-        case 6: return launch_l<6, PACK>(args, stream);
-        case 7: return launch_l<7, PACK>(args, stream);
-        case 8: return launch_l<8, PACK>(args, stream);
+        case 1: return launch_l<1, PACK, W64>(args, stream);
+        case 2: return launch_l<2, PACK, W64>(args, stream);
+        case 3: return launch_l<3, PACK, W64>(args, stream);
+        case 4: return launch_l<4, PACK, W64>(args, stream);
+        case 5: return launch_l<5, PACK, W64>(args, stream);
+        case 6: return launch_l<6, PACK, W64>(args, stream);
+        case 7: return launch_l<7, PACK, W64>(args, stream);
+        case 8: return launch_l<8, PACK, W64>(args, stream);
         default: return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core contraction: 1 <= l <= 8");
     }
 }
@@ -271,12 +333,41 @@ int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream) {
     if (args.B == 0) return TFHE_OK;
     if (args.npad % KTC_N || args.n_big % KTC_COEF || (args.B + KTC_M - 1) / KTC_M > 65535)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core contraction: unsupported shape");
+    const int limbs = args.w64 ? 8 : 4;
     if (args.pack_T > 0) {
-        if (!args.pack_out || args.npad != 8 * args.pack_N)
+        if (!args.pack_out || args.npad != limbs * 2 * args.pack_N)
             return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core packing: bad arguments");
-        return launch_any<true>(args, stream);
+        return args.w64 ? launch_any<true, true>(args, stream) : launch_any<true, false>(args, stream);
     }
-    return launch_any<false>(args, stream);
+    return args.w64 ? launch_any<false, true>(args, stream) : launch_any<false, false>(args, stream);
+}
+
+// 8-bit limb rows of a 64-bit key matrix (K rows, cols columns, row-major):
+// row 8 o + t, column k holds limb t of key[k][o] (signed, sum_t limb_t 2^(8t)
+// = key[k][o] mod 2^64); rows 8 cols .. npad - 1 are zero
+__global__ void limbs64_kernel(const unsigned long long* __restrict__ key, long long K, int cols, int npad,
+                               int8_t* __restrict__ limbs) {
+    const long long total = (long long)npad / 8 * K;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long o = idx / K;
+        const long long k = idx - o * K;
+        unsigned long long w = o < cols ? key[k * cols + o] : 0ULL;
+        for (int t = 0; t < 8; ++t) {
+            const int lo = (int)((w + 128ULL) & 255ULL) - 128;
+            limbs[(o * 8 + t) * K + k] = (int8_t)lo;
+            w = (w - (unsigned long long)(long long)lo) >> 8;
+        }
+    }
+}
+
+int build_limbs64(const unsigned long long* key, long long K, int cols, int npad, int8_t* limbs,
+                  cudaStream_t stream) {
+    const long long total = (long long)npad / 8 * K;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+    count_launch();
+    limbs64_kernel<<<blocks, 256, 0, stream>>>(key, K, cols, npad, limbs);
+    return check_cuda(cudaGetLastError(), "64-bit limb launch");
 }
 
 // limb rows of a packing key: row 4 o + t, o = poly * N + c, column k = i l + j

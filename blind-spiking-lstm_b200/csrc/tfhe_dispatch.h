@@ -11,6 +11,7 @@ using BrConvKernel = void (*)(const BskConvArgs);
 
 #define TFHE_DECLARE_LOGN(LG)                              \
     BrKernel br_fp64_logn_##LG(int L, bool reflayout, int kr, int kt, bool qtg, bool xt);     \
+    BrKernel br_fp64_t64_logn_##LG(int L, int kt, bool qtg, bool xt);                         \
     BrConvKernel bsk_fft_logn_##LG();
 
 TFHE_DECLARE_LOGN(7)
@@ -30,6 +31,19 @@ inline BrKernel br_fp64_kernel_for(int logn, int L, bool reflayout, int kr, int 
         case 10: return br_fp64_logn_10(L, reflayout, kr, kt, qtg, xt);
         case 11: return br_fp64_logn_11(L, reflayout, kr, kt, qtg, xt);
         case 12: return br_fp64_logn_12(L, reflayout, kr, kt, qtg, xt);
+        default: return nullptr;
+    }
+}
+
+// the T64 kernels (q = 2^64: uint64 LWEs, int64 LUTs, uint64 outputs)
+inline BrKernel br_fp64_t64_kernel_for(int logn, int L, int kt, bool qtg, bool xt) {
+    switch (logn) {
+        case 7: return br_fp64_t64_logn_7(L, kt, qtg, xt);
+        case 8: return br_fp64_t64_logn_8(L, kt, qtg, xt);
+        case 9: return br_fp64_t64_logn_9(L, kt, qtg, xt);
+        case 10: return br_fp64_t64_logn_10(L, kt, qtg, xt);
+        case 11: return br_fp64_t64_logn_11(L, kt, qtg, xt);
+        case 12: return br_fp64_t64_logn_12(L, kt, qtg, xt);
         default: return nullptr;
     }
 }
@@ -61,10 +75,14 @@ struct KsTcArgs {
     // pack_out (S, 2, pack_N); limb row 4 o + t with o = poly * N + coefficient
     int pack_T, pack_N;
     uint32_t* pack_out;
+    // 64-bit torus words (the pointers above then address uint64 words and
+    // the limb matrix has 8 rows per key column)
+    bool w64;
 };
 size_t ks_tc_smem_bytes(int l);
 int ks_tc_columns();
 int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream);
 int build_packing_limbs(const uint32_t* ksp, int n_dim, int l, int N, int8_t* limbs, cudaStream_t stream);
+int build_limbs64(const unsigned long long* key, long long K, int cols, int npad, int8_t* limbs, cudaStream_t stream);
 
 }  // namespace tfhe

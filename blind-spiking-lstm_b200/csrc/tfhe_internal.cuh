@@ -350,6 +350,16 @@ __device__ __forceinline__ void stage_all(double2* polys, int npoly, const doubl
     }
 }
 
+// rne(x / 2^s) of a centred 64-bit value, 1 <= s <= 63 (the reference's
+// round half to even, on the exact integer)
+__device__ __forceinline__ long long rne_div_pow2(long long x, int s) {
+    long long d = x >> s;
+    const unsigned long long low = (unsigned long long)x & ((1ULL << s) - 1ULL);
+    const unsigned long long half = 1ULL << (s - 1);
+    if (low > half || (low == half && (d & 1))) d += 1;
+    return d;
+}
+
 // ----------------------------------------------------------------------------
 // asynchronous 1D bulk copies into this CTA's own shared memory, and mbarriers
 // ----------------------------------------------------------------------------

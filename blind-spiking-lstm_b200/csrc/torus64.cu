@@ -873,6 +873,68 @@ int tfhe64_pack_lwes(const uint64_t* ksp, int32_t n_dim, int32_t N, int32_t log2
     return check_cuda(cudaGetLastError(), "packing64 launch");
 }
 
+int64_t tfhe64_tc_limb_rows(int32_t cols) {
+    if (cols < 1) return 0;
+    const long long rows = 8LL * cols;
+    const int tile = ks_tc_columns();
+    return (rows + tile - 1) / tile * tile;
+}
+
+int tfhe64_tc_limbs(const uint64_t* key, int64_t K, int32_t cols, int8_t* limbs, void* stream) {
+    if (!key || !limbs) return fail(TFHE_ERR_INVALID_ARGUMENT, "limbs64: null pointer");
+    if (K < 1 || cols < 1) return fail(TFHE_ERR_INVALID_ARGUMENT, "limbs64: bad sizes");
+    return build_limbs64(reinterpret_cast<const u64*>(key), K, cols, (int)tfhe64_tc_limb_rows(cols), limbs,
+                         (cudaStream_t)stream);
+}
+
+// the int32 sums of the tensor-core contraction cannot overflow: digits
+// |d| <= 2^(log2_beta - 1) <= 64, limbs |v| <= 128, K terms
+static bool tc_contraction_fits(long long K, int log2_beta) {
+    return log2_beta >= 1 && log2_beta <= 7 && K * (1LL << (log2_beta - 1)) * 128 < (1LL << 31);
+}
+
+int tfhe64_keyswitch_tc(const int8_t* limbs, int32_t n_big, int32_t n, int32_t l_ks, int32_t log2_beta_ks,
+                        const uint64_t* a_in, const uint64_t* b_in, uint64_t* a_out, uint64_t* b_out, int64_t batch,
+                        void* stream) {
+    if (n_big <= 0 || n <= 0 || n_big % 32) return fail(TFHE_ERR_INVALID_ARGUMENT, "keyswitch64 (tc): n_big % 32");
+    if (l_ks < 1 || l_ks > 8 || !tc_contraction_fits((long long)n_big * l_ks, log2_beta_ks))
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "keyswitch64 (tc): digits must fit 8 bits without int32 overflow");
+    if (batch < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "keyswitch64 (tc): negative batch");
+    if (batch == 0) return TFHE_OK;
+    if (!limbs || !a_in || !b_in || !a_out || !b_out) return fail(TFHE_ERR_INVALID_ARGUMENT, "keyswitch64 (tc): NULL");
+    if (reinterpret_cast<uintptr_t>(a_in) & 15) return fail(TFHE_ERR_INVALID_ARGUMENT, "keyswitch64 (tc): a_in alignment");
+    KsTcArgs args{reinterpret_cast<const uint32_t*>(a_in), reinterpret_cast<const uint32_t*>(b_in),
+                  reinterpret_cast<const unsigned char*>(limbs), n_big, n, l_ks, log2_beta_ks,
+                  (int)tfhe64_tc_limb_rows(n + 1), batch, reinterpret_cast<uint32_t*>(a_out),
+                  reinterpret_cast<uint32_t*>(b_out), WAIT_LIMIT_CYCLES, device_status_word(), 0, 0, nullptr, true};
+    if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
+    return launch_ks_tc(args, (cudaStream_t)stream);
+}
+
+int tfhe64_pack_lwes_tc(const int8_t* limbs, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
+                        const uint64_t* lwe_a, const uint64_t* lwe_b, int32_t T, int64_t S, uint64_t* out,
+                        void* stream) {
+    if (!valid_degree(N)) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing64 (tc): N must be a power of two");
+    if (l < 1 || l > 8 || n_dim < 32 || n_dim % 32 || !tc_contraction_fits((long long)n_dim * l, log2_beta))
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "packing64 (tc): n_dim % 32, digits in 8 bits, no int32 overflow");
+    if (T < 0 || T > N || S < 0) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing64 (tc): bad sizes (T <= N)");
+    if (S == 0) return TFHE_OK;
+    if (!limbs || !out || (T > 0 && (!lwe_a || !lwe_b))) return fail(TFHE_ERR_INVALID_ARGUMENT, "packing64 (tc): NULL");
+    if (T > 0 && (reinterpret_cast<uintptr_t>(lwe_a) & 15))
+        return fail(TFHE_ERR_INVALID_ARGUMENT, "packing64 (tc): lwe_a alignment");
+    const long long total = S * 2 * (long long)N;
+    count_launch();
+    pack_init64_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const u64*>(lwe_b), T, S,
+                                                                          N, reinterpret_cast<u64*>(out));
+    const int rc = check_cuda(cudaGetLastError(), "packing64 (tc) init launch");
+    if (rc != TFHE_OK || T == 0) return rc;
+    KsTcArgs args{reinterpret_cast<const uint32_t*>(lwe_a), nullptr, reinterpret_cast<const unsigned char*>(limbs),
+                  n_dim, 0, l, log2_beta, (int)tfhe64_tc_limb_rows(2 * N), S * T, nullptr, nullptr,
+                  WAIT_LIMIT_CYCLES, device_status_word(), T, N, reinterpret_cast<uint32_t*>(out), true};
+    if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
+    return launch_ks_tc(args, (cudaStream_t)stream);
+}
+
 int tfhe64_rlwe_rotate_add(const uint64_t* x, int32_t rot, const uint64_t* y, int64_t S, int32_t N, uint64_t* out,
                            void* stream) {
     if (!valid_degree(N)) return fail(TFHE_ERR_INVALID_ARGUMENT, "rotate/add64: N must be a power of two");

@@ -80,6 +80,9 @@ SIGNATURES = {
     "tfhe_fp32_keys_destroy": (None, [_P]),
     "tfhe_fp32_cuboot_merge": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _P, _I64, _I32, _P]),
     # the 64-bit torus (torus64.cu)
+    "tfhe64_keys_create": (ctypes.c_int, [ctypes.POINTER(TfheParams), _P, _P, ctypes.POINTER(_P)]),
+    "tfhe64_cuboot_merge": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _P, _I64, _P]),
+    "tfhe64_blind_rotate": (ctypes.c_int, [_P, _P, _P, _P, _I64, _I32, _P, _I64, _P]),
     "tfhe64_keyswitch": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _I64, _P]),
     "tfhe64_rotation_indices": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _I64, _P]),
     "tfhe64_rotate_extract": (ctypes.c_int, [_P, _P, _I32, _I32, _P, _P, _I64, _P]),
@@ -89,6 +92,10 @@ SIGNATURES = {
     "tfhe64_galois_keys_destroy": (ctypes.c_int, [_P]),
     "tfhe64_pack_lwe_to_rlwe": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P]),
     "tfhe64_pack_lwes": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _I32, _I64, _P, _P]),
+    "tfhe64_tc_limb_rows": (ctypes.c_int64, [_I32]),
+    "tfhe64_tc_limbs": (ctypes.c_int, [_P, _I64, _I32, _P, _P]),
+    "tfhe64_keyswitch_tc": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _I64, _P]),
+    "tfhe64_pack_lwes_tc": (ctypes.c_int, [_P, _I32, _I32, _I32, _I32, _P, _P, _I32, _I64, _P, _P]),
     "tfhe64_rlwe_rotate_add": (ctypes.c_int, [_P, _I32, _P, _I64, _I32, _P, _P]),
     "tfhe64_add": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "tfhe64_sample_extract": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I64, _P]),

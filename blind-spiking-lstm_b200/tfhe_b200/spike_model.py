@@ -55,9 +55,10 @@ def config_q64(**kw) -> SpikeModelConfig:
     """The layer on the reference's torus q = 2^64 with its bootstrapping
     parameters (N = 2048, n = 702, gadget 2^13 x 2, collapse 3, sigma 2^17),
     Galois key 2^8 x 5 (the reference's 40 bits, 2^2 x 20), packing key
-    2^8 x 4 (the reference's, parameters_crypto.py:18-20), inputs at
-    beta_x = 2^54."""
-    base = dict(log2_beta_x=54, gal_log2_beta=8, gal_l=5, pk_log2_beta=8, pk_l=4, sigma_rlwe=2.0 ** 17,
+    2^7 x 5 (35 bits where the reference keeps 32, parameters_crypto.py:18-20;
+    base 2^7 keeps the digits in int8, so the packing runs on the tensor
+    cores), inputs at beta_x = 2^54."""
+    base = dict(log2_beta_x=54, gal_log2_beta=8, gal_l=5, pk_log2_beta=7, pk_l=5, sigma_rlwe=2.0 ** 17,
                 pbs=client64.REF64, torus_bits=64)
     base.update(kw)
     return SpikeModelConfig(**base)

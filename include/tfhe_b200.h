@@ -341,9 +341,32 @@ int tfhe_fp32_cuboot_merge(const tfhe_fp32_keys* keys, const uint32_t* lwe_a, co
  * reference holds values in float64.  Torus values are uint64 words and
  * every integer step is exact modulo 2^64; gadget digits are the
  * reference's decomposition (schemas/polynomial_jax.py:90-111: round half
- * to even) evaluated exactly on the integer.  The blind rotation is
- * tfhe_mul_bootstrap at log2_q = 64 (its FP64 chain, as the reference's).
+ * to even) evaluated exactly on the integer.  The blind rotation is the
+ * FP64 chain at q = 2^64, as the reference's: natively (tfhe64_keys_create,
+ * tfhe64_cuboot_merge) or through tfhe_mul_bootstrap at log2_q = 64.
  * ---------------------------------------------------------------------- */
+
+/* Bootstrapping keys on Z/2^64 (KeyGen, schemas/RLWE_jax.py:162-197):
+ * params as for tfhe_keys_create with log2_q = 64 and l_bs <= 3; bsk_coeff
+ * (host) (2, 2, G M, l_bs, N) uint64 = RLWE encryptions of the collapsed
+ * CMux key as for tfhe_keys_create.  The key is converted to its FP64
+ * spectra on the device; free with tfhe_keys_destroy.  The key switch on
+ * this torus takes its key directly (tfhe64_keyswitch*). */
+int tfhe64_keys_create(const tfhe_params* params, const uint64_t* bsk_coeff, void* stream, tfhe_keys** keys_out);
+
+/* cuboot_merge (schemas/RLWE_jax.py:281-303) on Z/2^64 in one kernel: the
+ * rotation indices of multiply_seq_monomial from the masks (exact integer
+ * sums, round half to even), the collapsed CMux chain from ACC = lut, the
+ * rotation by X^(-b~) and the extraction of n_lut LWEs.  lwe_a (batch, n),
+ * lwe_b (batch) uint64; lut (lut_count, 2, N) int64, lut_count 1 or batch;
+ * n_lut a power of two <= N -> out_a (batch, n_lut, N), out_b (batch,
+ * n_lut) uint64.  tfhe64_blind_rotate: the rotated ACC (batch, 2, N)
+ * instead of the extraction. */
+int tfhe64_cuboot_merge(const tfhe_keys* keys, const uint64_t* lwe_a, const uint64_t* lwe_b, const int64_t* lut,
+                        int64_t lut_count, int32_t n_lut, uint64_t* out_a, uint64_t* out_b, int64_t batch,
+                        void* stream);
+int tfhe64_blind_rotate(const tfhe_keys* keys, const uint64_t* lwe_a, const uint64_t* lwe_b, const int64_t* lut,
+                        int64_t lut_count, int32_t n_lut, uint64_t* acc_out, int64_t batch, void* stream);
 
 /* key_switch_LWE (schemas/LWE_jax.py:97-117) on Z/2^64: ksk (n_big l_ks,
  * n + 1) uint64, row i l_ks + j = LWE(-s_big[i] q / beta^(j+1)) as n mask
@@ -400,6 +423,28 @@ int tfhe64_pack_lwe_to_rlwe(const tfhe64_galois_keys* keys, const uint64_t* lwe_
 int tfhe64_pack_lwes(const uint64_t* ksp, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
                      const uint64_t* lwe_a, const uint64_t* lwe_b, int32_t T, int64_t S, uint64_t* out,
                      void* stream);
+
+/* The key switch and the packing on Z/2^64 on the tcgen05 tensor cores
+ * (kind::i8): every 64-bit key word split into eight signed 8-bit limbs,
+ * int8 digits x limbs -> int32 sums recombined modulo 2^64 (exact: the sums
+ * cannot overflow, checked).  Needs log2_beta <= 7, n_big (n_dim) a multiple
+ * of 32 and 16-byte aligned masks.
+ *   tfhe64_tc_limb_rows(cols): rows of the limb matrix of a key with `cols`
+ *     columns (8 cols rounded up to the CTA tile);
+ *   tfhe64_tc_limbs: key (K, cols) uint64 row-major -> limbs (rows, K) int8
+ *     (the key switch: K = n_big l_ks, cols = n + 1; the packing key
+ *     (n_dim, l, 2, N): K = n_dim l, cols = 2N);
+ *   tfhe64_keyswitch_tc / tfhe64_pack_lwes_tc: tfhe64_keyswitch and
+ *     tfhe64_pack_lwes (key_switch_LWE, schemas/LWE_jax.py:97-117; packing,
+ *     schemas/text_jax.py:211-239) from those limbs, same results. */
+int64_t tfhe64_tc_limb_rows(int32_t cols);
+int tfhe64_tc_limbs(const uint64_t* key, int64_t K, int32_t cols, int8_t* limbs, void* stream);
+int tfhe64_keyswitch_tc(const int8_t* limbs, int32_t n_big, int32_t n, int32_t l_ks, int32_t log2_beta_ks,
+                        const uint64_t* a_in, const uint64_t* b_in, uint64_t* a_out, uint64_t* b_out,
+                        int64_t batch, void* stream);
+int tfhe64_pack_lwes_tc(const int8_t* limbs, int32_t n_dim, int32_t N, int32_t log2_beta, int32_t l,
+                        const uint64_t* lwe_a, const uint64_t* lwe_b, int32_t T, int64_t S, uint64_t* out,
+                        void* stream);
 
 /* out[s] = X^rot x[s] + y[s] (y may be NULL), out = x + y, and the LWEs of
  * coefficients 0 .. count-1 of RLWEs (rotate_ciphertext, sum_ciphertext_
