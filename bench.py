@@ -308,9 +308,9 @@ def lstm_summary(args, dev, steps=2, warmup=1, torus_bits=64):
     weights in [-7, 7], head) timed as extra keys of the PBS line: seq/s on
     device-resident inputs, end to end with the inputs copied from pinned
     host memory and the logits copied back inside the timed region, and the
-    plain FP64 per-gate form (one bootstrap launch per gate and sequence; on
-    the 2^32 torus also one ciphertext per CTA, no persistence or key
-    prefetch, key switch on CUDA cores) on the same model and inputs.
+    plain FP64 per-gate form (one bootstrap launch per gate and sequence,
+    one ciphertext per CTA, no persistence or key prefetch, key switch on
+    CUDA cores) on the same model and inputs.
     torus_bits 64: the reference's own modulus and bootstrapping parameters
     (q = 2^64, N = 2048, n = 702, gadget 2^13 x 2, collapse 3); 32: the
     config-1 parameters on q = 2^32."""

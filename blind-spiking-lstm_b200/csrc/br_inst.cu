@@ -1,6 +1,6 @@
 // Instantiations of the FP64 blind-rotation kernel for one degree.
 // Compiled once per BR_LOGN (7 .. 12) so the degrees build in parallel.
-#include "br_fp64.cuh"
+#include "br_split.cuh"
 #include "tfhe_dispatch.h"
 
 #ifndef BR_LOGN
@@ -55,5 +55,14 @@ BrKernel TFHE_CAT(br_fp64_logn_, BR_LOGN)(int L, bool reflayout, int kr, int kt,
 }
 
 BrConvKernel TFHE_CAT(bsk_fft_logn_, BR_LOGN)() { return bsk_fft_kernel<BR_LOGN>; }
+
+BrKernel TFHE_CAT(br_split_logn_, BR_LOGN)(int L) {
+    switch (L) {
+        case 1: return br_split_kernel<BR_LOGN, 1, false>;
+        case 2: return br_split_kernel<BR_LOGN, 2, false>;
+        case 3: return br_split_kernel<BR_LOGN, 3, false>;
+        default: return nullptr;
+    }
+}
 
 }  // namespace tfhe

@@ -1,8 +1,9 @@
 // Instantiations of the FP64 blind-rotation kernel on the 64-bit torus
 // (T64) for one degree, compiled once per BR_LOGN beside br_inst.cu.
 // Shapes: the one-CTA layout with extra threads, the quarter-root-table-in-
-// global layout, and the plain layout; l_bs 1 .. 3.
-#include "br_fp64.cuh"
+// global layout, and the plain layout; l_bs 1 .. 3; and the cluster-pair
+// kernel of small batches (br_split.cuh).
+#include "br_split.cuh"
 #include "tfhe_dispatch.h"
 
 #ifndef BR_LOGN
@@ -32,6 +33,15 @@ BrKernel TFHE_CAT(br_fp64_t64_logn_, BR_LOGN)(int L, int kt, bool qtg, bool xt) 
         default: return nullptr;
     }
 #undef TFHE_BR64_CASE
+}
+
+BrKernel TFHE_CAT(br_split64_logn_, BR_LOGN)(int L) {
+    switch (L) {
+        case 1: return br_split_kernel<BR_LOGN, 1, true>;
+        case 2: return br_split_kernel<BR_LOGN, 2, true>;
+        case 3: return br_split_kernel<BR_LOGN, 3, true>;
+        default: return nullptr;
+    }
 }
 
 }  // namespace tfhe

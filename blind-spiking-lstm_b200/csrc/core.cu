@@ -365,9 +365,98 @@ static int prepare_kernel(const void* kern, int nt, size_t smem, int* per_sm) {
     return TFHE_OK;
 }
 
+// One ciphertext per cluster of two CTAs (br_split.cuh) for batches that fit
+// in one wave of clusters.  TFHE_B200_SPLIT=0 turns it off; an explicitly
+// requested shape (tuning, TFHE_B200_K) never takes it.
+static bool split_enabled() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_SPLIT");
+        return !(env && env[0] == '0');
+    }();
+    return on;
+}
+
+static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, const tfhe_tuning* tune) {
+    const bool t64 = args.lwe_a64 != nullptr;
+    BrKernel kern = br_split_kernel_for(ilog2(N), L, t64);
+    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
+    const size_t smem = br_split_smem(N, L, args.M, br_table_bytes(N));
+    int per_sm = 1;
+    TFHE_TRY(prepare_kernel((const void*)kern, BR_SPLIT_THREADS, smem, &per_sm));
+    BrArgs a = args;
+    const FftPlan* pl = get_plan(N);
+    if (!pl) return TFHE_ERR_INTERNAL;
+    a.qt = pl->qt;
+    a.qr = pl->qr;
+    a.tw = pl->tw;
+    a.freq = pl->freq;
+    a.K = 1;
+    a.l2_prefetch = (tune && tune->l2_prefetch == 0) ? 0 : 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * args.B), 1, 1);
+    cfg.blockDim = dim3(BR_SPLIT_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    count_launch();
+    return check_cuda(cudaLaunchKernelEx(&cfg, kern, a), "blind rotation launch (cluster pair)");
+}
+
+// clusters of two that can be resident at once (a GPC with an odd number of
+// free SMs leaves one out), cached per device and kernel shape
+static long long split_resident_clusters(int N, int L, int M, bool t64) {
+    BrKernel kern = br_split_kernel_for(ilog2(N), L, t64);
+    if (!kern) return 0;
+    const size_t smem = br_split_smem(N, L, M, br_table_bytes(N));
+    if (smem > (size_t)max_smem_optin()) return 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, size_t>, long long> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_tuple(dev, (const void*)kern, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    long long n = 0;
+    if (cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * std::max(1, sm_count())), 1, 1);
+        cfg.blockDim = dim3(BR_SPLIT_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int c = 0;
+        if (cudaOccupancyMaxActiveClusters(&c, (const void*)kern, &cfg) == cudaSuccess) n = c;
+    }
+    cudaGetLastError();   // a refused query only disables the cluster form
+    cache.emplace(key, n);
+    return n;
+}
+
+static bool split_applies(int N, int L, int M, long long B, bool reflayout, int kr, const tfhe_tuning* tune,
+                          bool t64) {
+    const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
+    if (kr != 0 || reflayout || requested || L > 3 || !split_enabled() || B < 1 || 2 * B > sm_count()) return false;
+    return B <= split_resident_clusters(N, L, M, t64);
+}
+
 static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream,
                      int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
+    const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
+    if (split_applies(N, L, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
+        return launch_split(args, N, L, stream, tune);
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
                               : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0, !reflayout);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
@@ -416,7 +505,6 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
     // the small-batch shape (one ciphertext per CTA, 512 threads): that is
     // faster than a partly filled round of K ciphertexts per CTA (n=742
     // N=2048: 3.9 against 4.95 ms).  Not for explicitly requested shapes.
-    const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
     if (persistent && kr == 0 && sh.K > 1 && !requested && sets > grid) {
         const long long full = (sets / grid) * grid * sh.K;      // ciphertexts in whole rounds
         const long long rest = args.B - full;
@@ -1243,6 +1331,12 @@ int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* cipher
     *threads = sh.nt;
     *shared_bytes = (int64_t)sh.smem;
     return sh.K > 0 ? TFHE_OK : fail(TFHE_ERR_INVALID_ARGUMENT, "no launch shape fits");
+}
+
+int32_t tfhe_keys_cluster_size(const tfhe_keys* keys, int64_t batch) {
+    if (!keys) return 0;
+    const tfhe_params& p = keys->p;
+    return split_applies(p.N, p.l_bs, keys->M, batch, false, keys->ring_kr, &keys->tune, p.log2_q == 64) ? 2 : 1;
 }
 
 int64_t tfhe_launch_count(void) { return launch_count(); }

@@ -2,7 +2,7 @@
 // the FP64 blind-rotation kernels and the key-FFT kernel of its degree.
 #pragma once
 
-#include "br_fp64.cuh"
+#include "br_split.cuh"
 
 namespace tfhe {
 
@@ -12,6 +12,8 @@ using BrConvKernel = void (*)(const BskConvArgs);
 #define TFHE_DECLARE_LOGN(LG)                              \
     BrKernel br_fp64_logn_##LG(int L, bool reflayout, int kr, int kt, bool qtg, bool xt);     \
     BrKernel br_fp64_t64_logn_##LG(int L, int kt, bool qtg, bool xt);                         \
+    BrKernel br_split_logn_##LG(int L);                                                       \
+    BrKernel br_split64_logn_##LG(int L);                                                     \
     BrConvKernel bsk_fft_logn_##LG();
 
 TFHE_DECLARE_LOGN(7)
@@ -44,6 +46,19 @@ inline BrKernel br_fp64_t64_kernel_for(int logn, int L, int kt, bool qtg, bool x
         case 10: return br_fp64_t64_logn_10(L, kt, qtg, xt);
         case 11: return br_fp64_t64_logn_11(L, kt, qtg, xt);
         case 12: return br_fp64_t64_logn_12(L, kt, qtg, xt);
+        default: return nullptr;
+    }
+}
+
+// the cluster-pair kernels of small batches (one ciphertext per two CTAs)
+inline BrKernel br_split_kernel_for(int logn, int L, bool t64) {
+    switch (logn) {
+        case 7: return t64 ? br_split64_logn_7(L) : br_split_logn_7(L);
+        case 8: return t64 ? br_split64_logn_8(L) : br_split_logn_8(L);
+        case 9: return t64 ? br_split64_logn_9(L) : br_split_logn_9(L);
+        case 10: return t64 ? br_split64_logn_10(L) : br_split_logn_10(L);
+        case 11: return t64 ? br_split64_logn_11(L) : br_split_logn_11(L);
+        case 12: return t64 ? br_split64_logn_12(L) : br_split_logn_12(L);
         default: return nullptr;
     }
 }

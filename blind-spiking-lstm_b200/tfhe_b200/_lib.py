@@ -47,6 +47,7 @@ SIGNATURES = {
     "tfhe_keys_create_fourier": (ctypes.c_int, [ctypes.POINTER(TfheParams), _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "tfhe_keys_destroy": (None, [_P]),
     "tfhe_keys_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TfheTuning)]),
+    "tfhe_keys_cluster_size": (ctypes.c_int32, [_P, _I64]),
     "tfhe_keys_launch_shape": (ctypes.c_int, [_P, _I64, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
                                               ctypes.POINTER(_I64)]),
     "tfhe_keys_device_bytes": (_I64, [_P]),

@@ -148,6 +148,11 @@ class Keys:
                                                       ctypes.byref(sm)))
         return k.value, nt.value, sm.value
 
+    def cluster_size(self, batch: int) -> int:
+        """CTAs per ciphertext of a batch's blind rotation: 2 where one
+        ciphertext runs on a cluster pair (small batches), else 1."""
+        return int(_lib.load().tfhe_keys_cluster_size(self.handle, int(batch)))
+
     def device_bytes(self) -> int:
         return int(_lib.load().tfhe_keys_device_bytes(self.handle))
 

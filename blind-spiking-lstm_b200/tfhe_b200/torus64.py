@@ -59,6 +59,7 @@ class Keys64:
             self.bsk_dims = (ctypes.c_int64 * 6)(*self.bsk.shape)
         # the key switch on the tensor cores where its digits fit 8 bits
         self.ksk_limbs = _limbs(self.ksk, p.big * p.l_ks, p.n + 1) if _tc_ok(p.big, p.l_ks, p.log2_beta_ks) else None
+        self.ks_tensor_cores = -1
 
     def keyswitch(self, a, b, out_a=None, out_b=None, tensor_cores=-1, stream=None):
         """key_switch_LWE: on the tensor cores when the key has limbs and a is
@@ -70,6 +71,8 @@ class Keys64:
         out_a = out_a if out_a is not None else torch.empty((B, p.n), dtype=I64, device=a.device)
         out_b = out_b if out_b is not None else torch.empty((B,), dtype=I64, device=a.device)
         lib = _lib.load()
+        if tensor_cores < 0:
+            tensor_cores = self.ks_tensor_cores
         if self.ksk_limbs is not None and tensor_cores != 0 and a.data_ptr() % 16 == 0:
             _lib.check(lib.tfhe64_keyswitch_tc(_ptr(self.ksk_limbs), p.big, p.n, p.l_ks, p.log2_beta_ks, _ptr(a),
                                                _ptr(b), _ptr(out_a), _ptr(out_b), B, _stream(stream)))
@@ -77,6 +80,20 @@ class Keys64:
             _lib.check(lib.tfhe64_keyswitch(_ptr(self.ksk), p.big, p.n, p.l_ks, p.log2_beta_ks, _ptr(a), _ptr(b),
                                             _ptr(out_a), _ptr(out_b), B, _stream(stream)))
         return out_a, out_b
+
+    def set_tuning(self, ciphertexts_per_cta=0, prefetch=-1, persistent=-1, ks_tensor_cores=-1,
+                   l2_prefetch=-1) -> None:
+        """Launch shapes (speed only; 0 / -1: automatic), as Keys.set_tuning:
+        the blind rotation's ciphertexts per CTA, L1 prefetch, persistent
+        CTAs, L2 prefetch, and whether the key switch uses the tensor cores."""
+        t = _lib.TfheTuning(int(ciphertexts_per_cta), int(prefetch), int(persistent), int(ks_tensor_cores),
+                            int(l2_prefetch))
+        _lib.check(_lib.load().tfhe_keys_set_tuning(self.handle, ctypes.byref(t)))
+        self.ks_tensor_cores = int(ks_tensor_cores)
+
+    def cluster_size(self, batch: int) -> int:
+        """CTAs per ciphertext of a batch's blind rotation (2: cluster pair)."""
+        return int(_lib.load().tfhe_keys_cluster_size(self.handle, int(batch)))
 
     def close(self):
         if getattr(self, "handle", None):

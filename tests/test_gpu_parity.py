@@ -516,3 +516,33 @@ def test_keyswitch_unaligned_input_uses_cuda_cores():
     ga, gb = eng.keyswitch(a_view, device_u32(b.reshape(-1)))
     ra, rb = O.key_switch_LWE(k.ksk, (a, b), ks_params(name))
     assert np.array_equal(host_u32(ga), u32(ra)) and np.array_equal(host_u32(gb), u32(rb.reshape(-1)))
+
+
+@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2", "c1_N128", "c4_N4096"])
+def test_cluster_pair_kernel_matches_one_cta_kernel(name):
+    """Small batches run one ciphertext on a cluster of two CTAs (each owns
+    one ACC polynomial); the outputs are bit-identical to the one-CTA
+    kernel's (requested shape K = 1), at every parameter set, for the
+    extraction (n_lut 1 and 4) and for the rotated accumulator."""
+    p = PARAMS[name]
+    N = p["N"]
+    eng = engine(name)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for batch, n_lut in ((1, 1), (5, 4), (sms // 2, 1)):
+        msgs, a, b = inputs(name, batch, seed_offset=batch)
+        body = step_body(name) if n_lut == 1 else many_lut_body(name, n_lut)
+        lut = device_u32(np.stack([np.zeros(N), body])[None])
+        a_d, b_d = device_u32(a), device_u32(b.reshape(-1))
+        eng.set_tuning()
+        assert eng.cluster_size(batch) == 2
+        got = eng.pbs(a_d, b_d, lut, n_lut=n_lut)
+        ka, kb = eng.keyswitch(a_d, b_d)
+        acc = eng.blind_rotate(ka, kb, lut, n_lut=n_lut)
+        eng.set_tuning(ciphertexts_per_cta=1)
+        assert eng.cluster_size(batch) == 1
+        want = eng.pbs(a_d, b_d, lut, n_lut=n_lut)
+        acc1 = eng.blind_rotate(ka, kb, lut, n_lut=n_lut)
+        eng.set_tuning()
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (batch, n_lut)
+        assert torch.equal(acc, acc1), (batch, n_lut)
+    assert eng.cluster_size(sms // 2 + 1) == 1
