@@ -86,10 +86,10 @@ __device__ __forceinline__ void inverse_middle_one(double2* poly, const double2*
 }
 
 // shared memory of br_split_kernel: digit spectra [2][L][H], the output
-// polynomial [H], the tables, the rotation indices and b~
-inline size_t br_split_smem(int N, int L, int M, size_t table_bytes) {
+// polynomial [H], the tables, the rotation indices of every group and b~
+inline size_t br_split_smem(int N, int L, int G, int M, size_t table_bytes) {
     const int H = N / 2;
-    return (size_t)(2 * L + 1) * H * sizeof(double2) + table_bytes + (size_t)(M + 1) * sizeof(int) + 16;
+    return (size_t)(2 * L + 1) * H * sizeof(double2) + table_bytes + ((size_t)G * M + 1) * sizeof(int) + 16;
 }
 
 template <int LOGN, int L, bool T64>
@@ -109,8 +109,8 @@ __global__ void __launch_bounds__(BR_SPLIT_THREADS, 1) br_split_kernel(const BrA
     double2* qt_s = outp + H;                                // N / 2, swizzled
     double2* tw = qt_s + N / 2;                              // PL::TW
     uint16_t* freq = reinterpret_cast<uint16_t*>(tw + PL::TW);
-    int* rot = reinterpret_cast<int*>(freq + H);             // M
-    int* bexp = rot + M;                                     // 1
+    int* rot_all = reinterpret_cast<int*>(freq + H);         // G * M
+    int* bexp = rot_all + (size_t)args.G * M;                // 1
     auto qtab = [&](int r) { return qt_s[qsw<LOGN>(r)]; };
 
     const int tid = threadIdx.x;
@@ -157,6 +157,31 @@ __global__ void __launch_bounds__(BR_SPLIT_THREADS, 1) br_split_kernel(const BrA
 #pragma unroll
             for (int n2 = 0; n2 < 8; ++n2) acc_lo[n2] = acc_hi[n2] = 0.0;
         }
+        // rotation indices of every group of this ciphertext, up front (the
+        // formulas of br_fp64_kernel), so no group waits on a global load;
+        // read after the first group's barriers
+        for (int t = tid; t < args.G * M; t += nt) {
+            const int g = t / M, m = t - g * M;
+            int rr;
+            if constexpr (T64) {
+                unsigned long long v = 0ULL;
+                const unsigned long long* a = args.lwe_a64 + ct * args.lwe_n + (long long)g * args.collapse;
+                for (int c = 0; c < args.collapse; ++c)
+                    if ((m >> (args.collapse - 1 - c)) & 1) v += a[c];
+                const int ln = __ffs(args.n_lut) - 1;
+                const long long d = rne_div_pow2((long long)v, 63 - LOGN + ln);
+                rr = (int)((d << ln) & (2 * N - 1));
+            } else {
+                double v = 0.0;
+                const uint32_t* a = args.lwe_a + ct * args.lwe_n + (long long)g * args.collapse;
+                for (int c = 0; c < args.collapse; ++c)
+                    if ((m >> (args.collapse - 1 - c)) & 1) v += (double)(int32_t)a[c];
+                const double idx = rint((2.0 * N * v) / (q * args.n_lut)) * args.n_lut;
+                const int ri = (int)idx % (2 * N);
+                rr = ri < 0 ? ri + 2 * N : ri;
+            }
+            rot_all[t] = rr;
+        }
 
         for (int g = 0; g < args.G; ++g, ++step) {
             double2* mine_spec = spec + (size_t)(step & 1) * L * H;
@@ -174,28 +199,7 @@ __global__ void __launch_bounds__(BR_SPLIT_THREADS, 1) br_split_kernel(const BrA
                     prefetch_l2_bulk(base + off, (uint32_t)len);
                 }
             }
-            // rotation indices of this group (br_fp64_kernel's formulas)
-            for (int m = tid; m < M; m += nt) {
-                int rr;
-                if constexpr (T64) {
-                    unsigned long long v = 0ULL;
-                    const unsigned long long* a = args.lwe_a64 + ct * args.lwe_n + (long long)g * args.collapse;
-                    for (int c = 0; c < args.collapse; ++c)
-                        if ((m >> (args.collapse - 1 - c)) & 1) v += a[c];
-                    const int ln = __ffs(args.n_lut) - 1;
-                    const long long d = rne_div_pow2((long long)v, 63 - LOGN + ln);
-                    rr = (int)((d << ln) & (2 * N - 1));
-                } else {
-                    double v = 0.0;
-                    const uint32_t* a = args.lwe_a + ct * args.lwe_n + (long long)g * args.collapse;
-                    for (int c = 0; c < args.collapse; ++c)
-                        if ((m >> (args.collapse - 1 - c)) & 1) v += (double)(int32_t)a[c];
-                    const double idx = rint((2.0 * N * v) / (q * args.n_lut)) * args.n_lut;
-                    const int ri = (int)idx % (2 * N);
-                    rr = ri < 0 ? ri + 2 * N : ri;
-                }
-                rot[m] = rr;
-            }
+            const int* rot = rot_all + (size_t)g * M;
 
             // prologue: the digits of this CTA's polynomial, fold + twist,
             // first DIF superstage
@@ -277,25 +281,35 @@ __global__ void __launch_bounds__(BR_SPLIT_THREADS, 1) br_split_kernel(const BrA
                     double2 o = make_double2(0.0, 0.0);
                     const double2* kb2 = args.bsk + gbase + 2 * (size_t)p + (size_t)r * (P / 2) * M * H * 2;
                     // one ciphertext per SM leaves little to hide a key load's
-                    // latency behind: pattern m + 1's words are in flight while
-                    // pattern m is contracted (same operations, same order)
-                    double2 k[P], kn[P];
-#pragma unroll
-                    for (int jj = 0; jj < P / 2; ++jj) ldg_pair(kb2 + (size_t)jj * M * H * 2, k[2 * jj], k[2 * jj + 1]);
+                    // latency behind: the key words of MC patterns are all in
+                    // flight before the first of them is contracted (the
+                    // contraction keeps the pattern order: same operations,
+                    // same order as the one-CTA kernel)
+                    constexpr int MC = (8 / P) >= 4 ? 4 : ((8 / P) >= 2 ? 2 : 1);
 #pragma unroll 1
-                    for (int m = 0; m < M; ++m) {
-                        if (m + 1 < M) {
+                    for (int m0 = 0; m0 < M; m0 += MC) {
+                        double2 k[MC][P];
 #pragma unroll
-                            for (int jj = 0; jj < P / 2; ++jj)
-                                ldg_pair(kb2 + ((size_t)jj * M + m + 1) * H * 2, kn[2 * jj], kn[2 * jj + 1]);
-                        }
-                        const double2 w = root2n<LOGN, true>(qt_s, rot[m] * e);
-                        double2 t = make_double2(0.0, 0.0);
+                        for (int mc = 0; mc < MC; ++mc)
+                            if (m0 + mc < M) {
 #pragma unroll
-                        for (int bc = 0; bc < P; ++bc) c_mac(t, k[bc], d[bc]);
-                        c_mac(o, w, t);
+                                for (int jj = 0; jj < P / 2; ++jj)
+                                    ldg_pair(kb2 + ((size_t)jj * M + m0 + mc) * H * 2, k[mc][2 * jj],
+                                             k[mc][2 * jj + 1]);
+                            }
 #pragma unroll
-                        for (int bc = 0; bc < P; ++bc) k[bc] = kn[bc];
+                        for (int mc = 0; mc < MC; ++mc)
+                            if (m0 + mc < M) {
+                                double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+                                for (int bc = 0; bc < P; ++bc) c_mac(t, k[mc][bc], d[bc]);
+                                if (m0 + mc == 0) {
+                                    o = t;            // pattern 0 rotates by X^0 (as the one-CTA kernel)
+                                } else {
+                                    const double2 w = root2n<LOGN, true>(qt_s, rot[m0 + mc] * e);
+                                    c_mac(o, w, t);
+                                }
+                            }
                     }
                     outp[swz(p)] = o;
                 }

@@ -254,6 +254,14 @@ static int k_override() {
     return v;
 }
 
+static bool qtg_single() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_QTG1");
+        return env && env[0] == '1';
+    }();
+    return on;
+}
+
 static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0, bool allow_qtg = false) {
     const int H = N / 2, Q8 = H / 8;
     const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
@@ -302,6 +310,18 @@ static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0, boo
                     s.smem = smem2;
                     s.kt = 2;
                     s.qtg = true;
+                } else if (qtg_single() && kreq <= 0) {
+                    // two CTAs of one ciphertext each (experimental, TFHE_B200_QTG1=1)
+                    const size_t smem1 = per_ct + br_table_bytes(N) - (size_t)(N / 2) * sizeof(double2) +
+                                         (size_t)(M + 1) * sizeof(int) + 16;
+                    if (2 * (smem1 + 1024) <= (size_t)max_smem_per_sm()) {
+                        s.K = 1;
+                        s.nt = 2 * Q8;
+                        s.xt = false;
+                        s.smem = smem1;
+                        s.kt = 1;
+                        s.qtg = true;
+                    }
                 }
             }
             return s;
@@ -380,7 +400,7 @@ static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, c
     const bool t64 = args.lwe_a64 != nullptr;
     BrKernel kern = br_split_kernel_for(ilog2(N), L, t64);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
-    const size_t smem = br_split_smem(N, L, args.M, br_table_bytes(N));
+    const size_t smem = br_split_smem(N, L, args.G, args.M, br_table_bytes(N));
     int per_sm = 1;
     TFHE_TRY(prepare_kernel((const void*)kern, BR_SPLIT_THREADS, smem, &per_sm));
     BrArgs a = args;
@@ -410,10 +430,10 @@ static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, c
 
 // clusters of two that can be resident at once (a GPC with an odd number of
 // free SMs leaves one out), cached per device and kernel shape
-static long long split_resident_clusters(int N, int L, int M, bool t64) {
+static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
     BrKernel kern = br_split_kernel_for(ilog2(N), L, t64);
     if (!kern) return 0;
-    const size_t smem = br_split_smem(N, L, M, br_table_bytes(N));
+    const size_t smem = br_split_smem(N, L, G, M, br_table_bytes(N));
     if (smem > (size_t)max_smem_optin()) return 0;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
@@ -444,18 +464,18 @@ static long long split_resident_clusters(int N, int L, int M, bool t64) {
     return n;
 }
 
-static bool split_applies(int N, int L, int M, long long B, bool reflayout, int kr, const tfhe_tuning* tune,
-                          bool t64) {
+static bool split_applies(int N, int L, int G, int M, long long B, bool reflayout, int kr,
+                          const tfhe_tuning* tune, bool t64) {
     const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
     if (kr != 0 || reflayout || requested || L > 3 || !split_enabled() || B < 1 || 2 * B > sm_count()) return false;
-    return B <= split_resident_clusters(N, L, M, t64);
+    return B <= split_resident_clusters(N, L, G, M, t64);
 }
 
 static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream,
                      int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
     const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
-    if (split_applies(N, L, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
+    if (split_applies(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
         return launch_split(args, N, L, stream, tune);
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
                               : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0, !reflayout);
@@ -1336,7 +1356,9 @@ int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* cipher
 int32_t tfhe_keys_cluster_size(const tfhe_keys* keys, int64_t batch) {
     if (!keys) return 0;
     const tfhe_params& p = keys->p;
-    return split_applies(p.N, p.l_bs, keys->M, batch, false, keys->ring_kr, &keys->tune, p.log2_q == 64) ? 2 : 1;
+    return split_applies(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, p.log2_q == 64)
+               ? 2
+               : 1;
 }
 
 int64_t tfhe_launch_count(void) { return launch_count(); }

@@ -718,7 +718,8 @@ int tfhe_pack_lwes_with_key(const tfhe_packing_key* key, const uint32_t* lwe_a, 
     const int rc = check_cuda(cudaGetLastError(), "packing init launch");
     if (rc != TFHE_OK) return rc;
     KsTcArgs a{lwe_a, nullptr, reinterpret_cast<const unsigned char*>(key->limbs), key->n_dim, 0, key->l,
-               key->log2_beta, 8 * N, S * T, nullptr, nullptr, WAIT_LIMIT_CYCLES, device_status_word(), T, N, out};
+               key->log2_beta, 8 * N, S * T, nullptr, nullptr, WAIT_LIMIT_CYCLES, device_status_word(), T, N, out,
+               false, true};
     return launch_ks_tc(a, (cudaStream_t)stream);
 }
 

@@ -93,6 +93,9 @@ struct KsTcArgs {
     // 64-bit torus words (the pointers above then address uint64 words and
     // the limb matrix has 8 rows per key column)
     bool w64;
+    // the call may allocate stream-ordered scratch (the digit matrix the
+    // pipelined kernel reads by TMA); false: digits computed in the kernel
+    bool allow_alloc;
 };
 size_t ks_tc_smem_bytes(int l);
 int ks_tc_columns();

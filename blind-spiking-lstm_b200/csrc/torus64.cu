@@ -906,7 +906,8 @@ int tfhe64_keyswitch_tc(const int8_t* limbs, int32_t n_big, int32_t n, int32_t l
     KsTcArgs args{reinterpret_cast<const uint32_t*>(a_in), reinterpret_cast<const uint32_t*>(b_in),
                   reinterpret_cast<const unsigned char*>(limbs), n_big, n, l_ks, log2_beta_ks,
                   (int)tfhe64_tc_limb_rows(n + 1), batch, reinterpret_cast<uint32_t*>(a_out),
-                  reinterpret_cast<uint32_t*>(b_out), WAIT_LIMIT_CYCLES, device_status_word(), 0, 0, nullptr, true};
+                  reinterpret_cast<uint32_t*>(b_out), WAIT_LIMIT_CYCLES, device_status_word(), 0, 0, nullptr, true,
+                  true};
     if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
     return launch_ks_tc(args, (cudaStream_t)stream);
 }
@@ -930,7 +931,7 @@ int tfhe64_pack_lwes_tc(const int8_t* limbs, int32_t n_dim, int32_t N, int32_t l
     if (rc != TFHE_OK || T == 0) return rc;
     KsTcArgs args{reinterpret_cast<const uint32_t*>(lwe_a), nullptr, reinterpret_cast<const unsigned char*>(limbs),
                   n_dim, 0, l, log2_beta, (int)tfhe64_tc_limb_rows(2 * N), S * T, nullptr, nullptr,
-                  WAIT_LIMIT_CYCLES, device_status_word(), T, N, reinterpret_cast<uint32_t*>(out), true};
+                  WAIT_LIMIT_CYCLES, device_status_word(), T, N, reinterpret_cast<uint32_t*>(out), true, true};
     if (!args.status) return fail(TFHE_ERR_INTERNAL, "device status word unavailable");
     return launch_ks_tc(args, (cudaStream_t)stream);
 }
