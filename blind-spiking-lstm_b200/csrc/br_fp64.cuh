@@ -501,18 +501,9 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                                 }
                             }
                         }
-                        // pattern 0 (no LWE term) always rotates by X^0: its
-                        // product with w = 1 is the contraction itself, so the
-                        // kernel adds it directly (the same sums as c_mac with
-                        // w = 1, up to the sign of zeros)
-                        const bool first = !REFLAYOUT && m == 0;
                         double2 w[KT];
 #pragma unroll
                         for (int kt = 0; kt < KT; ++kt) {
-                            if (first) {
-                                w[kt] = make_double2(1.0, 0.0);
-                                continue;
-                            }
                             const int r = rot[(kg * KT + kt) * M + m];
                             if constexpr (REFLAYOUT) {
                                 w[kt] = __ldg(args.all_rot + (size_t)r * H + jr);
@@ -551,13 +542,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                             }
 #pragma unroll
                             for (int kt = 0; kt < KT; ++kt) {
-                                if (first) {
-                                    o0[kt] = t0[kt];
-                                    o1[kt] = t1[kt];
-                                } else {
-                                    c_mac(o0[kt], w[kt], t0[kt]);
-                                    c_mac(o1[kt], w[kt], t1[kt]);
-                                }
+                                c_mac(o0[kt], w[kt], t0[kt]);
+                                c_mac(o1[kt], w[kt], t1[kt]);
                             }
                         } else {
                             // one output at a time: P key words in flight
@@ -583,14 +569,8 @@ __global__ void __launch_bounds__(KR > 0 ? KR * (1 << LOGN) / 8 : 512, 1) br_fp6
                                 }
 #pragma unroll
                                 for (int kt = 0; kt < KT; ++kt) {
-                                    if (first) {
-                                        if (a == 0) o0[kt] = t[kt];
-                                        else o1[kt] = t[kt];
-                                    } else if (a == 0) {
-                                        c_mac(o0[kt], w[kt], t[kt]);
-                                    } else {
-                                        c_mac(o1[kt], w[kt], t[kt]);
-                                    }
+                                    if (a == 0) c_mac(o0[kt], w[kt], t[kt]);
+                                    else c_mac(o1[kt], w[kt], t[kt]);
                                 }
                             }
                         }

@@ -303,12 +303,8 @@ __global__ void __launch_bounds__(BR_SPLIT_THREADS, 1) br_split_kernel(const BrA
                                 double2 t = make_double2(0.0, 0.0);
 #pragma unroll
                                 for (int bc = 0; bc < P; ++bc) c_mac(t, k[mc][bc], d[bc]);
-                                if (m0 + mc == 0) {
-                                    o = t;            // pattern 0 rotates by X^0 (as the one-CTA kernel)
-                                } else {
-                                    const double2 w = root2n<LOGN, true>(qt_s, rot[m0 + mc] * e);
-                                    c_mac(o, w, t);
-                                }
+                                const double2 w = root2n<LOGN, true>(qt_s, rot[m0 + mc] * e);
+                                c_mac(o, w, t);
                             }
                     }
                     outp[swz(p)] = o;

@@ -254,14 +254,6 @@ static int k_override() {
     return v;
 }
 
-static bool qtg_single() {
-    static const bool on = [] {
-        const char* env = getenv("TFHE_B200_QTG1");
-        return env && env[0] == '1';
-    }();
-    return on;
-}
-
 static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0, bool allow_qtg = false) {
     const int H = N / 2, Q8 = H / 8;
     const size_t per_ct = (size_t)2 * L * H * sizeof(double2);
@@ -310,18 +302,6 @@ static BrShape br_shape(int N, int L, int M, long long B, int k_request = 0, boo
                     s.smem = smem2;
                     s.kt = 2;
                     s.qtg = true;
-                } else if (qtg_single() && kreq <= 0) {
-                    // two CTAs of one ciphertext each (experimental, TFHE_B200_QTG1=1)
-                    const size_t smem1 = per_ct + br_table_bytes(N) - (size_t)(N / 2) * sizeof(double2) +
-                                         (size_t)(M + 1) * sizeof(int) + 16;
-                    if (2 * (smem1 + 1024) <= (size_t)max_smem_per_sm()) {
-                        s.K = 1;
-                        s.nt = 2 * Q8;
-                        s.xt = false;
-                        s.smem = smem1;
-                        s.kt = 1;
-                        s.qtg = true;
-                    }
                 }
             }
             return s;
