@@ -52,6 +52,15 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
     return ((uint64_t)hi << 32) | lo;
 }
 
+// K-major descriptor of a tile written by TMA with 32-byte swizzling: rows of
+// 32 bytes (one MMA's K), 8-row atoms 256 bytes apart; the leading byte
+// offset is unused for swizzled K-major layouts; layout type 6 = 32B swizzle
+__device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t saddr) {
+    const uint32_t lo = ((saddr >> 4) & 0x3FFFu) | (1u << 16);
+    const uint32_t hi = ((256u >> 4) & 0x3FFFu) | (1u << 14) | (6u << 29);
+    return ((uint64_t)hi << 32) | lo;
+}
+
 // instruction descriptor: D s32, A and B signed 8-bit, both K-major
 constexpr uint32_t KTC_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(KTC_N >> 3) << 17) |
                                ((uint32_t)(KTC_M >> 4) << 24);
@@ -456,7 +465,9 @@ __device__ __forceinline__ void store_cols(const KsTcArgs& a, long long row, int
     }
 }
 
-template <int L, bool PACK, bool W64, bool A_TMA>
+// SW: TMA copies of 32-byte K slices with 32-byte swizzling (one copy per
+// MMA K step, whole 32-byte sectors) instead of 16-byte chunks
+template <int L, bool PACK, bool W64, bool A_TMA, bool SW>
 __global__ void __launch_bounds__(KT2_THREADS, 1)
     ks_tc2_kernel(const KsTcArgs a, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   int rows_fast) {
@@ -513,10 +524,20 @@ __global__ void __launch_bounds__(KT2_THREADS, 1)
                 unsigned char* st = smem_raw + (size_t)slot * (A_BYTES + B_BYTES);
                 mbar_arrive_expect_tx(&full[slot], B_BYTES + (A_TMA ? A_BYTES : 0u));
                 const int x0 = s * KTC_COEF * L;
+                if constexpr (SW) {
 #pragma unroll 1
-                for (int c = 0; c < CH; ++c) {
-                    tma_load_2d(st + A_BYTES + c * KTC_N * 16, &tmB, x0 + c * 16, col0, &full[slot]);
-                    if constexpr (A_TMA) tma_load_2d(st + c * KTC_M * 16, &tmA, x0 + c * 16, (int)row0, &full[slot]);
+                    for (int kk = 0; kk < L; ++kk) {
+                        tma_load_2d(st + A_BYTES + kk * KTC_N * 32, &tmB, x0 + kk * 32, col0, &full[slot]);
+                        if constexpr (A_TMA)
+                            tma_load_2d(st + kk * KTC_M * 32, &tmA, x0 + kk * 32, (int)row0, &full[slot]);
+                    }
+                } else {
+#pragma unroll 1
+                    for (int c = 0; c < CH; ++c) {
+                        tma_load_2d(st + A_BYTES + c * KTC_N * 16, &tmB, x0 + c * 16, col0, &full[slot]);
+                        if constexpr (A_TMA)
+                            tma_load_2d(st + c * KTC_M * 16, &tmA, x0 + c * 16, (int)row0, &full[slot]);
+                    }
                 }
                 issued = s + 1;
             }
@@ -536,9 +557,13 @@ __global__ void __launch_bounds__(KT2_THREADS, 1)
                 const uint32_t sa = smem_addr(smem_raw + (size_t)slot * (A_BYTES + B_BYTES));
                 const uint32_t sb = sa + A_BYTES;
 #pragma unroll
-                for (int kk = 0; kk < L; ++kk)     // K = 32 bytes = chunks 2 kk, 2 kk + 1
-                    mma_i8(tmem, smem_desc(sa + 2 * kk * KTC_M * 16, KTC_M * 16, 128),
-                           smem_desc(sb + 2 * kk * KTC_N * 16, KTC_N * 16, 128), (s > 0 || kk > 0) ? 1u : 0u);
+                for (int kk = 0; kk < L; ++kk) {   // K = 32 bytes = chunks 2 kk, 2 kk + 1
+                    const uint64_t da = (SW && A_TMA) ? smem_desc_sw32(sa + kk * KTC_M * 32)
+                                                      : smem_desc(sa + 2 * kk * KTC_M * 16, KTC_M * 16, 128);
+                    const uint64_t db = SW ? smem_desc_sw32(sb + kk * KTC_N * 32)
+                                           : smem_desc(sb + 2 * kk * KTC_N * 16, KTC_N * 16, 128);
+                    mma_i8(tmem, da, db, (s > 0 || kk > 0) ? 1u : 0u);
+                }
                 mma_commit(&empty[slot]);
             }
             mma_commit(&done);              // arrives once every MMA issued above has completed
@@ -646,19 +671,29 @@ static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
 
 // (rows, K) int8 matrix, row-major with K bytes per row; boxes of one 16-byte
 // K chunk x box_rows rows; rows past the end read as zero
-static int make_chunk_map(CUtensorMap* m, const void* base, long long K, long long rows, int box_rows) {
+static int make_chunk_map(CUtensorMap* m, const void* base, long long K, long long rows, int box_rows, bool sw) {
     const PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
     if (!enc) return fail(TFHE_ERR_INTERNAL, "tensor-core contraction: cuTensorMapEncodeTiled unavailable");
     if ((reinterpret_cast<uintptr_t>(base) & 15) || K % 16)
         return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core contraction: operand not 16-byte aligned");
     const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)K};
-    const cuuint32_t box[2] = {16u, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {sw ? 32u : 16u, (cuuint32_t)box_rows};
     const cuuint32_t es[2] = {1u, 1u};
     const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, es,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, sw ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? TFHE_OK : fail(TFHE_ERR_INTERNAL, "tensor-core contraction: tensor map encoding failed");
+}
+
+// TFHE_B200_TC_SW=0: 16-byte chunk copies without swizzling (for comparison)
+static bool tc_swizzle() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_TC_SW");
+        return !(env && env[0] == '0');
+    }();
+    return on;
 }
 
 template <int L, bool PACK, bool W64>
@@ -670,7 +705,8 @@ static int launch_l2(const KsTcArgs& args, cudaStream_t stream) {
     if ((rows_fast ? ct : rt) > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "tensor-core contraction: too many tiles");
     CUtensorMap ta, tb;
     memset(&ta, 0, sizeof(ta));
-    int rc = make_chunk_map(&tb, args.limbs, K, args.npad, KTC_N);
+    const bool sw = tc_swizzle();
+    int rc = make_chunk_map(&tb, args.limbs, K, args.npad, KTC_N, sw);
     if (rc != TFHE_OK) return rc;
     int8_t* dig = nullptr;
     if (args.allow_alloc) {
@@ -681,11 +717,12 @@ static int launch_l2(const KsTcArgs& args, cudaStream_t stream) {
         tc_digits_kernel<L, W64><<<(unsigned)std::min<long long>((words + 255) / 256, 148LL * 16), 256, 0, stream>>>(
             args.a_in, args.B, args.n_big, args.log2_beta, dig);
         rc = check_cuda(cudaGetLastError(), "digit matrix launch");
-        if (rc == TFHE_OK) rc = make_chunk_map(&ta, dig, K, args.B, KTC_M);
+        if (rc == TFHE_OK) rc = make_chunk_map(&ta, dig, K, args.B, KTC_M, sw);
     }
     if (rc == TFHE_OK) {
         const size_t smem = (size_t)kt2_stages(L) * kt2_stage_bytes(L);
-        auto kern = dig ? ks_tc2_kernel<L, PACK, W64, true> : ks_tc2_kernel<L, PACK, W64, false>;
+        auto kern = dig ? (sw ? ks_tc2_kernel<L, PACK, W64, true, true> : ks_tc2_kernel<L, PACK, W64, true, false>)
+                        : (sw ? ks_tc2_kernel<L, PACK, W64, false, true> : ks_tc2_kernel<L, PACK, W64, false, false>);
         rc = tc_set_smem_once((const void*)kern, smem);
         if (rc == TFHE_OK) {
             const dim3 grid = rows_fast ? dim3((unsigned)rt, (unsigned)ct) : dim3((unsigned)ct, (unsigned)rt);

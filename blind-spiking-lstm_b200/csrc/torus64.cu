@@ -27,6 +27,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <string>
 
 #include "tfhe_b200.h"
@@ -501,6 +502,136 @@ __global__ void __launch_bounds__(TRACE_NT) trace64_kernel(const Trace64Args arg
     }
 }
 
+// The same trace with the four limbs' products transformed back together:
+// the pointwise stage writes all 2 x LIMBS output spectra, one inverse pass
+// runs over the eight polynomials (every thread busy, a quarter of the
+// barriers), and the accumulators live in the registers of the threads that
+// own their coefficients (thread i: coefficients i and i + H of its slots),
+// the permuted copies passing through the spectra's space.  Every value is
+// computed by trace64_kernel's operations in the same order, so the outputs
+// are identical.  Shared memory: (l + 2 LIMBS) H complex values.
+template <int LOGN>
+__global__ void __launch_bounds__(TRACE_NT) trace64_fused_kernel(const Trace64Args args) {
+    constexpr int N = 1 << LOGN;
+    constexpr int H = N / 2;
+    constexpr int LOGH = LOGN - 1;
+    constexpr int SL = H >= TRACE_NT ? H / TRACE_NT : 1;     // coefficient slots per thread
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* dig = reinterpret_cast<double2*>(smem_raw);        // l * H
+    double2* res = dig + (size_t)args.l * H;                     // 2 LIMBS * H
+    u64* permA = reinterpret_cast<u64*>(res);                    // N (in res, before the products)
+    u64* permB = permA + N;                                      // N
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long r = blockIdx.x;
+    constexpr double inv_h = 1.0 / H;
+
+    u64 accA[SL][2], accB[SL][2];
+    const u64* a = args.lwe_a + r * N;
+#pragma unroll
+    for (int sl = 0; sl < SL; ++sl) {
+        const int i = tid + sl * nt;
+#pragma unroll
+        for (int hf = 0; hf < 2; ++hf) {
+            accA[sl][hf] = accB[sl][hf] = 0ULL;
+            if (i >= H) continue;
+            const int c = i + hf * H;
+            long long rm;
+            const u64 ms = (u64)rne_shift((long long)a[c == 0 ? 0 : N - c], LOGN, &rm);
+            accA[sl][hf] = c == 0 ? ms : 0ULL - ms;
+            accB[sl][hf] = c == 0 ? (u64)rne_shift((long long)args.lwe_b[r], LOGN, &rm) : 0ULL;
+        }
+    }
+
+    for (int st = 0; st < args.steps; ++st) {
+        const int k = (1 << (args.steps - st)) + 1;
+        // automorphism X -> X^k of the owned coefficients, into shared memory
+#pragma unroll
+        for (int sl = 0; sl < SL; ++sl) {
+            const int i = tid + sl * nt;
+            if (i >= H) continue;
+#pragma unroll
+            for (int hf = 0; hf < 2; ++hf) {
+                const int j = i + hf * H;
+                const int dst = (int)(((long long)j * k) % (2 * N));
+                const int t = dst % N;
+                permA[t] = dst >= N ? 0ULL - accA[sl][hf] : accA[sl][hf];
+                permB[t] = dst >= N ? 0ULL - accB[sl][hf] : accB[sl][hf];
+            }
+        }
+        __syncthreads();
+        // gadget digits of A', fold + twist; B' of the owned coefficients kept
+        u64 pB[SL][2];
+#pragma unroll
+        for (int sl = 0; sl < SL; ++sl) {
+            const int i = tid + sl * nt;
+            pB[sl][0] = pB[sl][1] = 0ULL;
+            if (i >= H) continue;
+            pB[sl][0] = permB[i];
+            pB[sl][1] = permB[i + H];
+            long long xl = (long long)permA[i], xh = (long long)permA[i + H];
+            const double2 w = args.qt[i];
+            for (int lvl = 0; lvl < args.l; ++lvl) {
+                const int sh = 64 - (lvl + 1) * args.log2_beta;
+                long long rl, rh;
+                const double dl = (double)rne_shift(xl, sh, &rl);
+                const double dh = (double)rne_shift(xh, sh, &rh);
+                xl = rl;
+                xh = rh;
+                dig[(size_t)lvl * H + swz(i)] = make_double2(fma(w.x, dl, w.y * dh), fma(w.y, dl, -w.x * dh));
+            }
+        }
+        __syncthreads();
+        fwd<LOGH, 0>(dig, args.l, args.tw, tid, nt);
+        const double2* key = args.key + (size_t)st * args.l * 2 * LIMBS * H;
+        for (int p = tid; p < H; p += nt) {
+            for (int limb = 0; limb < LIMBS; ++limb) {
+                double2 o0 = make_double2(0.0, 0.0), o1 = make_double2(0.0, 0.0);
+                for (int lvl = 0; lvl < args.l; ++lvl) {
+                    const double2 d = dig[(size_t)lvl * H + swz(p)];
+                    c_mac(o0, d, key[(((size_t)lvl * 2 + 0) * LIMBS + limb) * H + p]);
+                    c_mac(o1, d, key[(((size_t)lvl * 2 + 1) * LIMBS + limb) * H + p]);
+                }
+                res[(size_t)(2 * limb) * H + swz(p)] = o0;
+                res[(size_t)(2 * limb + 1) * H + swz(p)] = o1;
+            }
+        }
+        __syncthreads();
+        inv<LOGH, Plan<LOGH>::NS - 1>(res, 2 * LIMBS, args.tw, tid, nt);
+#pragma unroll
+        for (int sl = 0; sl < SL; ++sl) {
+            const int i = tid + sl * nt;
+            if (i >= H) continue;
+            const double2 w = c_conj(args.qt[i]);
+            u64 ka0 = 0ULL, ka1 = 0ULL, kb0 = 0ULL, kb1 = 0ULL;
+#pragma unroll
+            for (int limb = 0; limb < LIMBS; ++limb) {
+                const double2 ua = c_mul(w, res[(size_t)(2 * limb) * H + swz(i)]);
+                const double2 ub = c_mul(w, res[(size_t)(2 * limb + 1) * H + swz(i)]);
+                const int sh = 16 * limb;
+                ka0 += (u64)(long long)rint(ua.x * inv_h) << sh;
+                ka1 += (u64)(long long)rint(-ua.y * inv_h) << sh;
+                kb0 += (u64)(long long)rint(ub.x * inv_h) << sh;
+                kb1 += (u64)(long long)rint(-ub.y * inv_h) << sh;
+            }
+            accA[sl][0] += ka0;
+            accA[sl][1] += ka1;
+            accB[sl][0] += pB[sl][0] + kb0;
+            accB[sl][1] += pB[sl][1] + kb1;
+        }
+        __syncthreads();
+    }
+    u64* dst = args.out + r * 2 * N;
+#pragma unroll
+    for (int sl = 0; sl < SL; ++sl) {
+        const int i = tid + sl * nt;
+        if (i >= H) continue;
+        dst[i] = accA[sl][0];
+        dst[i + H] = accA[sl][1];
+        dst[N + i] = accB[sl][0];
+        dst[N + i + H] = accB[sl][1];
+    }
+}
+
 // ---------------------------------------------------------------- packing
 constexpr int PK_TB = 64, PK_TO = 64, PK_KC = 4, PK_LMAX = 8;
 
@@ -653,14 +784,33 @@ size_t trace_smem(int N, int l) {
     return (size_t)(l + 2) * (N / 2) * sizeof(double2) + 4 * (size_t)N * sizeof(u64);
 }
 
+size_t trace_fused_smem(int N, int l) { return (size_t)(l + 2 * LIMBS) * (N / 2) * sizeof(double2); }
+
+// the fused-limb kernel where its spectra fit in shared memory
+// (TFHE_B200_TRACE_FUSED=0: the limb-by-limb kernel, for comparison)
+static bool trace_fused_enabled() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_TRACE_FUSED");
+        return !(env && env[0] == '0');
+    }();
+    return on;
+}
+
 template <int LOGN>
 int launch_trace(const Trace64Args& a, long long R, cudaStream_t stream) {
-    const size_t smem = trace_smem(1 << LOGN, a.l);
-    const cudaError_t e =
-        cudaFuncSetAttribute(trace64_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        optin = 0;
+    const size_t fsmem = trace_fused_smem(1 << LOGN, a.l);
+    const bool fused = trace_fused_enabled() && fsmem <= (size_t)optin;
+    const size_t smem = fused ? fsmem : trace_smem(1 << LOGN, a.l);
+    const void* kern = fused ? (const void*)trace64_fused_kernel<LOGN> : (const void*)trace64_kernel<LOGN>;
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "trace (2^64) attribute");
     count_launch();
-    trace64_kernel<LOGN><<<(unsigned)R, TRACE_NT, smem, stream>>>(a);
+    if (fused) trace64_fused_kernel<LOGN><<<(unsigned)R, TRACE_NT, smem, stream>>>(a);
+    else trace64_kernel<LOGN><<<(unsigned)R, TRACE_NT, smem, stream>>>(a);
     return check_cuda(cudaGetLastError(), "trace (2^64) launch");
 }
 

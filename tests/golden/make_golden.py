@@ -19,6 +19,7 @@ Run from the repository root with REFERENCE_ROOT naming a checkout of the
 reference (the output is committed and the tests never read the reference):
 
     REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_golden.py
+    REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_golden.py cfg2
 """
 from __future__ import annotations
 
@@ -93,9 +94,13 @@ PARAMS = {
                     sigma_glwe=1.0, sigma_lwe=2.0 ** 15),
     "cfg1": dict(q=Q, N=1024, n=630, beta_bs=2 ** 7, l_bs=3, collapse=3, beta_ks=2 ** 3, l_ks=5,
                  sigma_glwe=2.0 ** 7, sigma_lwe=2.0 ** 17),
+    # config 2 of the PBS workload (n=742, N=2048, beta 2^15 x 2, KS 2^4 x 5,
+    # collapse 2): written to its own file by `make_golden.py cfg2`
+    "cfg2": dict(q=Q, N=2048, n=742, beta_bs=2 ** 15, l_bs=2, collapse=2, beta_ks=2 ** 4, l_ks=5,
+                 sigma_glwe=1.0, sigma_lwe=2.0 ** 15),
 }
-KEY_SEED = {"tiny_c3": 11, "tiny_c2": 12, "cfg1": 13}
-INPUT_SEED = {"tiny_c3": 21, "tiny_c2": 22, "cfg1": 23}
+KEY_SEED = {"tiny_c3": 11, "tiny_c2": 12, "cfg1": 13, "cfg2": 14}
+INPUT_SEED = {"tiny_c3": 21, "tiny_c2": 22, "cfg1": 23, "cfg2": 24}
 
 
 def special_values():
@@ -136,13 +141,13 @@ def gen_polynomial(out):
     out["plain_lut_n4"] = lut
 
 
-def gen_pbs(name, out, n_lut_list=(1,), batch=4):
+def gen_pbs(name, out, n_lut_list=(1,), batch=4, t=32, t_out=32):
+    """Messages in Z_{t/2} at q/t; the step LUT's output at q/t_out."""
     p = PARAMS[name]
     N, q = p["N"], p["q"]
     keys = O.keygen(p, KEY_SEED[name])
     rng = np.random.default_rng(INPUT_SEED[name])
-    t = 32
-    msgs = rng.integers(0, 16, size=batch)
+    msgs = rng.integers(0, t // 2, size=batch)
     a, b = O.encrypt_inputs(keys, msgs, q / t, rng)
     out[f"{name}_in_a"], out[f"{name}_in_b"], out[f"{name}_msgs"] = a, b, msgs
     ks_params = {"beta_ks": p["beta_ks"], "l_ks": p["l_ks"], "q": q}
@@ -154,7 +159,7 @@ def gen_pbs(name, out, n_lut_list=(1,), batch=4):
     all_rot = keys.all_rot
     for n_lut in n_lut_list:
         if n_lut == 1:
-            body = O.step_lut(N, 16, 8, q / t)
+            body = O.step_lut(N, t // 2, t // 4, q / t_out)
         else:
             s = 4.0
             body = sum(np.asarray(get_plain_LUT_ref(N, n_lut, i, s, g))
@@ -170,7 +175,7 @@ def gen_pbs(name, out, n_lut_list=(1,), batch=4):
                     all_rot, n_lut)
         out[f"{name}_br{n_lut}"] = np.asarray(acc)
     # pure-JAX bootstrapping path (rotation before), as test_collapse.py:173
-    body = O.step_lut(N, 16, 8, q / t)
+    body = O.step_lut(N, t // 2, t // 4, q / t_out)
     luts = [np.zeros((batch, N)), np.broadcast_to(body, (batch, N)).copy()]
     ba, bb = vmap(RJ.bootstrapping, in_axes=(0, 0, None, None, None, None, None, None, None))(
         (ca, cb), luts, keys.bsk_ordered, q, p["beta_bs"], p["l_bs"], N, p["collapse"], all_rot)
@@ -198,5 +203,20 @@ def main():
     print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
 
 
+def main_cfg2():
+    """Config 2 (gadget 2^15, where the reference's FP64 products round):
+    four ciphertexts of Z_8 (at q/16) through the reference's key switch,
+    cuboot_merge and BR, the step LUT's output at q/8 (its noise, ~2^25,
+    needs that margin)."""
+    out = {}
+    gen_pbs("cfg2", out, n_lut_list=(1,), batch=4, t=16, t_out=8)
+    path = os.path.join(HERE, "pbs_cfg2_golden.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["cfg2"]:
+        main_cfg2()
+    else:
+        main()

@@ -155,7 +155,7 @@ def test_beta15_against_exact_product(name, batch):
     assert np.array_equal(dec_x, (msgs >= 4).astype(float))
 
 
-@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "c1_N128", "c4_N4096", "cfg1"])
+@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "c1_N128", "c4_N4096", "cfg1", "cfg2"])
 def test_one_group_against_exact(name):
     """One CMux group through tfhe_mul_bootstrap (reference layout) against
     the exact integer product: max error bounded, bit-exact when beta <= 2^8."""
@@ -546,3 +546,34 @@ def test_cluster_pair_kernel_matches_one_cta_kernel(name):
         assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (batch, n_lut)
         assert torch.equal(acc, acc1), (batch, n_lut)
     assert eng.cluster_size(sms // 2 + 1) == 1
+
+
+def test_cfg2_against_reference_golden():
+    """Config 2 through the engine against the reference's own key switch
+    and cuboot_merge (tests/golden/pbs_cfg2_golden.npz, generated by
+    make_golden.py cfg2): the key switch bit for bit; the bootstrap by
+    decryption and by phase, each output within 2^27 of its value (decision
+    margin q/16 = 2^28), on the one-CTA and the cluster-pair kernels."""
+    import os
+    G2 = np.load(os.path.join(os.path.dirname(__file__), "golden", "pbs_cfg2_golden.npz"))
+    name = "cfg2"
+    p = PARAMS[name]
+    q, N = p["q"], p["N"]
+    k = keys(name)
+    eng = engine(name)
+    a_d, b_d = device_u32(G2["cfg2_in_a"]), device_u32(G2["cfg2_in_b"].reshape(-1))
+    ka, kb = eng.keyswitch(a_d, b_d)
+    assert np.array_equal(host_u32(ka), u32(G2["cfg2_ks_a"]))
+    assert np.array_equal(host_u32(kb), u32(G2["cfg2_ks_b"].reshape(-1)))
+    lut = device_u32(np.stack([np.zeros(N), G2["cfg2_lut1"]])[None])
+    want = (G2["cfg2_msgs"] >= 4).astype(np.float64)
+    sk = k.sk_glwe.astype(np.float64)
+    for cpc in (0, 1):                     # automatic (cluster pair at this batch), one CTA per ciphertext
+        eng.set_tuning(ciphertexts_per_cta=cpc)
+        oa, ob = eng.pbs(a_d, b_d, lut)
+        oa = centred(host_u32(oa))[:, 0].astype(np.float64)
+        ob = centred(host_u32(ob))[:, 0].astype(np.float64)
+        ph = np.mod(ob - oa @ sk + q / 2, q) - q / 2
+        assert np.array_equal(np.rint(ph / (q / 8)), want), cpc
+        assert np.abs(ph - want * q / 8).max() <= 2.0 ** 27, cpc
+    eng.set_tuning()

@@ -183,3 +183,38 @@ def test_all_rot_table_matches_reference_digest():
     np.testing.assert_array_equal(arr[[0, 1, 2047, 2048, 4095]], G["allrot2048_rows"])
     digest = np.frombuffer(hashlib.sha256(arr.tobytes()).digest(), dtype=np.uint8)
     assert np.array_equal(digest, G["allrot2048_sha256"])
+
+
+G2 = np.load(os.path.join(HERE, "golden", "pbs_cfg2_golden.npz"))
+CFG2 = dict(q=Q, N=2048, n=742, beta_bs=2 ** 15, l_bs=2, collapse=2, beta_ks=2 ** 4, l_ks=5,
+            sigma_glwe=1.0, sigma_lwe=2.0 ** 15)
+
+
+def test_pbs_golden_cfg2():
+    """Config 2 (n=742, N=2048, gadget 2^15 x 2, collapse 2) against the
+    reference's own key switch and cuboot_merge (tests/golden/make_golden.py
+    cfg2): the key switch bit for bit; the bootstrap, where gadget 2^15
+    makes both FP64 chains round, by decryption (Z_8 inputs at q/16, the step
+    LUT's output at q/8) and by phase: each output within 2^27 of its value
+    (the decision margin is q/16 = 2^28; measured noise ~2^25)."""
+    from pbs_cases import keys as case_keys
+    p = CFG2
+    k = case_keys("cfg2")
+    q, N = p["q"], p["N"]
+    rng = np.random.default_rng(24)
+    msgs = rng.integers(0, 8, size=4)
+    a, b = O.encrypt_inputs(k, msgs, q / 16, rng)
+    assert np.array_equal(msgs, G2["cfg2_msgs"])
+    assert np.array_equal(a, G2["cfg2_in_a"]) and np.array_equal(b, G2["cfg2_in_b"])
+    ca, cb = O.key_switch_LWE(k.ksk, (a, b), {"beta_ks": p["beta_ks"], "l_ks": p["l_ks"], "q": q})
+    assert np.array_equal(ca, G2["cfg2_ks_a"]) and np.array_equal(cb, G2["cfg2_ks_b"])
+    body = G2["cfg2_lut1"]
+    enc = [np.zeros((4, N)), np.broadcast_to(body, (4, N))]
+    acc = O.BR((ca, cb), enc, k.bsk_ordered, q, p["beta_bs"], p["l_bs"], N, p["collapse"], k.all_rot, 1)
+    ra, rb = O.extract_many(acc, 1)
+    want = (msgs >= 4).astype(np.float64)
+    sk = k.sk_glwe.astype(np.float64)
+    for oa, ob in ((ra, rb), (G2["cfg2_merge1_a"], G2["cfg2_merge1_b"])):
+        assert np.array_equal(O.decrypt_LWE((oa[:, 0], ob[:, 0]), k.sk_glwe, {"t": 8, "q": q}), want)
+        ph = np.mod(np.asarray(ob[:, 0, 0], np.float64) - np.asarray(oa[:, 0], np.float64) @ sk + q / 2, q) - q / 2
+        assert np.abs(ph - want * q / 8).max() <= 2.0 ** 27
