@@ -262,6 +262,8 @@ def run_engine(args, rank, world, local_rank, dist):
         torch.cuda.empty_cache()
         lstm = lstm_summary(args, dev, steps=1, warmup=1, torus_bits=64)
         lstm_q32 = lstm_summary(args, dev, torus_bits=32)
+        torch.cuda.empty_cache()
+        serving = serving_summary(args)
 
     total = B * args.steps * world
     value = total / (dev_ms * 1e-3)
@@ -299,7 +301,27 @@ def run_engine(args, rank, world, local_rank, dist):
     if lstm is not None:
         line["lstm"] = lstm
         line["lstm_q32"] = lstm_q32
+        line["serving"] = serving
     return line
+
+
+def serving_summary(args):
+    """Config 5 as extra keys of the default line: the serving run of
+    --serve (Poisson arrivals at 2 requests/s, 24 requests of U[8, 64]
+    Zipf(1.1) tokens, 2 layers of hidden 256 on the 2^32 torus, continuous
+    batching), reduced to its latency percentiles and throughput."""
+    import argparse
+    sargs = argparse.Namespace(**vars(args))
+    sargs.rate, sargs.requests, sargs.torus, sargs.hidden, sargs.layers = 2.0, 24, 32, 128, 1
+    sargs.warmup = 1
+    out = run_serve(sargs)
+    return {"workload": "Spike-LSTM serving (config 5): Poisson 2 req/s, 24 requests of U[8,64] tokens, "
+                        f"{out['config']['layers']} layers x hidden {out['config']['hidden']}, "
+                        f"PBS {out['config']['pbs']}, {out['config']['torus']}",
+            "p50_s": out["latency"]["p50_s"], "p99_s": out["latency"]["p99_s"],
+            "seq_per_s": out["value"], "tokens_per_s": out["tokens_per_s"], "mean_batch": out["mean_batch"],
+            "one_at_a_time_seq_per_s": out["one_at_a_time"]["seq_per_s"],
+            "results_equal_to_one_at_a_time": out["one_at_a_time"]["results_equal_to_mix"]}
 
 
 def lstm_summary(args, dev, steps=2, warmup=1, torus_bits=64):
