@@ -1,6 +1,7 @@
 // Instantiations of the FP64 blind-rotation kernel for one degree.
 // Compiled once per BR_LOGN (7 .. 12) so the degrees build in parallel.
 #include "br_split.cuh"
+#include "br_tm.cuh"
 #include "tfhe_dispatch.h"
 
 #ifndef BR_LOGN
@@ -64,5 +65,15 @@ BrKernel TFHE_CAT(br_split_logn_, BR_LOGN)(int L) {
         default: return nullptr;
     }
 }
+
+#if BR_LOGN == 11
+BrKernel br_tm32_logn11(int L) {
+    switch (L) {
+        case 1: return br_tm_kernel<11, 1, 3, false>;
+        case 2: return br_tm_kernel<11, 2, 3, false>;
+        default: return nullptr;
+    }
+}
+#endif
 
 }  // namespace tfhe

@@ -4,6 +4,7 @@
 // global layout, and the plain layout; l_bs 1 .. 3; and the cluster-pair
 // kernel of small batches (br_split.cuh).
 #include "br_split.cuh"
+#include "br_tm.cuh"
 #include "tfhe_dispatch.h"
 
 #ifndef BR_LOGN
@@ -43,5 +44,15 @@ BrKernel TFHE_CAT(br_split64_logn_, BR_LOGN)(int L) {
         default: return nullptr;
     }
 }
+
+#if BR_LOGN == 11
+BrKernel br_tm64_logn11(int L) {
+    switch (L) {
+        case 1: return br_tm_kernel<11, 1, 3, true>;
+        case 2: return br_tm_kernel<11, 2, 3, true>;
+        default: return nullptr;
+    }
+}
+#endif
 
 }  // namespace tfhe

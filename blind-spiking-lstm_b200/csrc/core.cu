@@ -451,12 +451,82 @@ static bool split_applies(int N, int L, int G, int M, long long B, bool reflayou
     return B <= split_resident_clusters(N, L, G, M, t64);
 }
 
+// the arguments of ciphertexts full .. B - 1 of a launch
+static BrArgs args_after(const BrArgs& args, long long full, int N) {
+    BrArgs tail = args;
+    tail.B = args.B - full;
+    if (tail.lwe_a) tail.lwe_a += full * args.lwe_n;
+    if (tail.lwe_b) tail.lwe_b += full;
+    if (tail.lut) tail.lut += full * args.lut_stride;
+    if (tail.ct_init) tail.ct_init += full * args.ct_stride;
+    if (tail.indices) tail.indices += full * (long long)args.G * args.M;
+    if (tail.acc_out) tail.acc_out += full * 2 * N;
+    if (tail.out_a) tail.out_a += full * args.n_lut * N;
+    if (tail.out_b) tail.out_b += full * args.n_lut;
+    if (tail.out_i64) tail.out_i64 += full * 2 * N;
+    if (tail.lwe_a64) tail.lwe_a64 += full * args.lwe_n;
+    if (tail.lwe_b64) tail.lwe_b64 += full;
+    if (tail.lut64) tail.lut64 += full * args.lut_stride;
+    if (tail.acc_out64) tail.acc_out64 += full * 2 * N;
+    if (tail.out_a64) tail.out_a64 += full * args.n_lut * N;
+    if (tail.out_b64) tail.out_b64 += full * args.n_lut;
+    return tail;
+}
+
+// Three ciphertexts per CTA with the accumulators in tensor memory
+// (br_tm.cuh) at N = 2048, l_bs <= 2: requested with ciphertexts_per_cta = 3,
+// or automatic when TFHE_B200_TM=1; whole rounds of 3 x SMs ciphertexts go to
+// it, the rest to the launch shapes below.
+static bool tm_default() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_TM");
+        return env && env[0] == '1';
+    }();
+    return on;
+}
+
+static int launch_tm(const BrArgs& args, int N, int L, cudaStream_t stream, const tfhe_tuning* tune,
+                     long long full) {
+    const bool t64 = args.lwe_a64 != nullptr;
+    BrKernel kern = br_tm_kernel_for(ilog2(N), L, t64);
+    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
+    const size_t smem = br_tm_smem(N, L, 3, args.M, br_table_bytes(N));
+    int per_sm = 1;
+    TFHE_TRY(prepare_kernel((const void*)kern, BR_TM_THREADS, smem, &per_sm));
+    BrArgs a = args;
+    const FftPlan* pl = get_plan(N);
+    if (!pl) return TFHE_ERR_INTERNAL;
+    a.qt = pl->qt;
+    a.qr = pl->qr;
+    a.tw = pl->tw;
+    a.freq = pl->freq;
+    a.K = 3;
+    a.B = full;
+    a.l2_prefetch = (tune && tune->l2_prefetch == 0) ? 0 : 1;
+    count_launch();
+    kern<<<(unsigned)sm_count(), BR_TM_THREADS, smem, stream>>>(a);
+    return check_cuda(cudaGetLastError(), "blind rotation launch (tensor memory)");
+}
+
 static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStream_t stream,
                      int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
     const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
     if (split_applies(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
         return launch_split(args, N, L, stream, tune);
+    if (!reflayout && kr == 0 && N == 2048 && L <= 2 &&
+        ((tune && tune->ciphertexts_per_cta == 3) || (!requested && tm_default())) &&
+        br_tm_smem(N, L, 3, args.M, br_table_bytes(N)) <= (size_t)max_smem_optin()) {
+        const long long round = 3LL * sm_count();
+        const long long full = (args.B / round) * round;
+        if (full > 0) {
+            TFHE_TRY(launch_tm(args, N, L, stream, tune, full));
+            if (full == args.B) return TFHE_OK;
+            tfhe_tuning rest_tune = tune ? *tune : tfhe_tuning{0, -1, -1, -1, -1};
+            if (rest_tune.ciphertexts_per_cta == 3) rest_tune.ciphertexts_per_cta = 0;
+            return launch_br(args_after(args, full, N), N, L, reflayout, kr, stream, status, &rest_tune);
+        }
+    }
     const BrShape sh = kr > 0 ? ring_shape(N, L, args.M)
                               : br_shape(N, L, args.M, args.B, tune ? tune->ciphertexts_per_cta : 0, !reflayout);
     if (kr > 0 && sh.kr != kr) return fail(TFHE_ERR_INVALID_ARGUMENT, "key ring layout not available for these keys");
@@ -514,24 +584,7 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
             count_launch();
             kern<<<(unsigned)grid, sh.nt, sh.smem, stream>>>(head);
             TFHE_TRY(check_cuda(cudaGetLastError(), "blind rotation launch"));
-            BrArgs tail = args;
-            tail.B = rest;
-            if (tail.lwe_a) tail.lwe_a += full * args.lwe_n;
-            if (tail.lwe_b) tail.lwe_b += full;
-            if (tail.lut) tail.lut += full * args.lut_stride;
-            if (tail.ct_init) tail.ct_init += full * args.ct_stride;
-            if (tail.indices) tail.indices += full * (long long)args.G * args.M;
-            if (tail.acc_out) tail.acc_out += full * 2 * N;
-            if (tail.out_a) tail.out_a += full * args.n_lut * N;
-            if (tail.out_b) tail.out_b += full * args.n_lut;
-            if (tail.out_i64) tail.out_i64 += full * 2 * N;
-            if (tail.lwe_a64) tail.lwe_a64 += full * args.lwe_n;
-            if (tail.lwe_b64) tail.lwe_b64 += full;
-            if (tail.lut64) tail.lut64 += full * args.lut_stride;
-            if (tail.acc_out64) tail.acc_out64 += full * 2 * N;
-            if (tail.out_a64) tail.out_a64 += full * args.n_lut * N;
-            if (tail.out_b64) tail.out_b64 += full * args.n_lut;
-            return launch_br(tail, N, L, reflayout, 0, stream, status, tune);
+            return launch_br(args_after(args, full, N), N, L, reflayout, 0, stream, status, tune);
         }
     }
     count_launch();

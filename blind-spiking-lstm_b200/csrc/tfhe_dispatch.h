@@ -3,6 +3,7 @@
 #pragma once
 
 #include "br_split.cuh"
+#include "br_tm.cuh"
 
 namespace tfhe {
 
@@ -61,6 +62,14 @@ inline BrKernel br_split_kernel_for(int logn, int L, bool t64) {
         case 12: return t64 ? br_split64_logn_12(L) : br_split_logn_12(L);
         default: return nullptr;
     }
+}
+
+// the tensor-memory kernels (three ciphertexts per CTA), N = 2048 only
+BrKernel br_tm32_logn11(int L);
+BrKernel br_tm64_logn11(int L);
+inline BrKernel br_tm_kernel_for(int logn, int L, bool t64) {
+    if (logn != 11) return nullptr;
+    return t64 ? br_tm64_logn11(L) : br_tm32_logn11(L);
 }
 
 inline BrConvKernel bsk_fft_kernel_for(int logn) {

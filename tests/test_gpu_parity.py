@@ -577,3 +577,29 @@ def test_cfg2_against_reference_golden():
         assert np.array_equal(np.rint(ph / (q / 8)), want), cpc
         assert np.abs(ph - want * q / 8).max() <= 2.0 ** 27, cpc
     eng.set_tuning()
+
+
+def test_tensor_memory_kernel_matches_two_per_cta():
+    """Three ciphertexts per CTA with the accumulators in tensor memory
+    (ciphertexts_per_cta = 3, N = 2048) give the outputs of the two-per-CTA
+    kernel bit for bit; the batch leaves a remainder after the whole rounds
+    of 3 x SMs, which runs on the other shapes."""
+    name = "cfg2"
+    p = PARAMS[name]
+    N = p["N"]
+    eng = engine(name)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    batch = 3 * sms + 37
+    msgs, a, b = inputs(name, batch, seed_offset=7)
+    lut = device_u32(np.stack([np.zeros(N), many_lut_body(name, 2)])[None])
+    a_d, b_d = device_u32(a), device_u32(b.reshape(-1))
+    ka, kb = eng.keyswitch(a_d, b_d)
+    eng.set_tuning(ciphertexts_per_cta=3)
+    got = eng.pbs(a_d, b_d, lut, n_lut=2)
+    acc = eng.blind_rotate(ka, kb, lut, n_lut=2)
+    eng.set_tuning(ciphertexts_per_cta=2)
+    want = eng.pbs(a_d, b_d, lut, n_lut=2)
+    acc2 = eng.blind_rotate(ka, kb, lut, n_lut=2)
+    eng.set_tuning()
+    assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+    assert torch.equal(acc, acc2)

@@ -173,6 +173,23 @@ def test_cluster_pair_kernel_matches_one_cta_kernel64():
         assert torch.equal(acc, acc1), (B, n_lut)
 
 
+def test_tensor_memory_kernel_matches_two_per_cta64():
+    """The tensor-memory kernel (three ciphertexts per CTA) on the 64-bit
+    torus at the reference's parameters: bit-identical to two per CTA."""
+    p = C64.REF64
+    ck, dk, ok = keys_for(p)
+    rng = np.random.default_rng(46)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    B = 3 * sms + 11
+    lut_d, a_d, b_d = d64(rnd(rng, B, 2, p.N)), d64(rnd(rng, B, p.n)), d64(rnd(rng, B))
+    dk.set_tuning(ciphertexts_per_cta=3)
+    got = dk.cuboot_merge(a_d, b_d, lut_d, 4)
+    dk.set_tuning(ciphertexts_per_cta=2)
+    want = dk.cuboot_merge(a_d, b_d, lut_d, 4)
+    dk.set_tuning()
+    assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+
+
 def test_64bit_keys_refuse_32bit_entry_points():
     from tfhe_b200 import _lib
     ck, dk, ok = keys_for(SMALL)
