@@ -296,16 +296,19 @@ __global__ void __launch_bounds__(KTC_THREADS, 1) ks_tc_kernel(KsTcArgs a) {
 // ============================================================================
 // Pipelined form: operands fed by the Tensor Memory Accelerator.
 //
-// The limb key tile (B) of every stage arrives by 2D TMA copies (one 16-byte
-// K chunk x 256 limb rows per copy, no multicast, a tensor map over this
-// GPU's memory only) into a ring of stages; the digits (A) either arrive the
+// The limb key tile (B) of every stage arrives by 2D TMA copies (one 32-byte
+// K slice x 256 limb rows per copy with 32-byte swizzling, or one 16-byte
+// chunk unswizzled; each CTA fetches its own tiles, through a tensor map over
+// this GPU's memory only) into a ring of stages; the digits (A) either arrive the
 // same way from a digit matrix made once per call (tc_digits_kernel) or are
 // computed by 8 producer warps into the ring.  One thread issues the copies,
 // one thread the MMAs; full / empty mbarriers per stage pass the ring between
 // them, so loads of stage s + 1 .. s + S - 1 overlap the MMAs of stage s.
-// Shared layout per stage and operand: [chunk][row][16 B] (a 16-byte K chunk
-// of all rows contiguous), i.e. the K-major no-swizzle canonical layout with
-// leading byte offset rows * 16 and stride byte offset 128.
+// Shared layout per stage and operand: with swizzling, [slice][row][32 B]
+// (one 32-byte K slice of all rows, 8-row atoms of 256 bytes, the descriptor's
+// 32-byte swizzle mode); without, and for digits the producers write,
+// [chunk][row][16 B], the K-major no-swizzle canonical layout with leading
+// byte offset rows * 16 and stride byte offset 128.
 // ============================================================================
 constexpr int KT2_THREADS = 384;               // warp 0: copies, warp 1: MMAs, warps 4-11: digits + epilogue
 constexpr uint32_t KT2_SMEM_BUDGET = 200 * 1024;
