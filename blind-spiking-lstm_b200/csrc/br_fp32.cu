@@ -341,9 +341,7 @@ static size_t smem_bytes(int N, int L, int K, int M) {
 template <int LOGN, int L, int K>
 static int launch_br(const Args& a, cudaStream_t stream) {
     const size_t smem = smem_bytes(1 << LOGN, L, K, a.M);
-    const cudaError_t e = cudaFuncSetAttribute(br_fp32_kernel<LOGN, L, K>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "fp32 blind rotation attribute");
+    TFHE_TRY(smem_attr_once((const void*)br_fp32_kernel<LOGN, L, K>, smem));
     const long long grid = (a.B + K - 1) / K;
     count_launch();
     br_fp32_kernel<LOGN, L, K><<<(unsigned)grid, NT, smem, stream>>>(a);

@@ -53,11 +53,6 @@ int check_cuda(cudaError_t e, const char* what) {
     return fail(TFHE_ERR_INTERNAL, msg);
 }
 
-#define TFHE_TRY(expr)                          \
-    do {                                        \
-        const int _rc = (expr);                 \
-        if (_rc != TFHE_OK) return _rc;         \
-    } while (0)
 
 // ---------------------------------------------------------------- FFT plans
 static int ilog2(long long v) {
@@ -343,6 +338,21 @@ static BrShape ring_shape(int N, int L, int M) {
 static std::mutex g_attr_mu;
 static std::map<std::pair<int, const void*>, int> g_attr_smem;
 static std::map<std::tuple<int, const void*, int, size_t>, int> g_occupancy;
+
+// the dynamic shared-memory attribute of a kernel, raised once per device
+// and size (later launches make no attribute call, and can be captured)
+int smem_attr_once(const void* kern, size_t smem) {
+    int dev = 0;
+    TFHE_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    int& have = g_attr_smem[{dev, kern}];
+    if (have < (int)smem) {
+        TFHE_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(dynamic shared memory)"));
+        have = (int)smem;
+    }
+    return TFHE_OK;
+}
 
 static int prepare_kernel(const void* kern, int nt, size_t smem, int* per_sm) {
     int dev = 0;

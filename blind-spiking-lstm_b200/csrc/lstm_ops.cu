@@ -498,8 +498,7 @@ int max_smem() {
 template <int LOGN>
 int launch_trace(const TraceArgs& a, long long R, size_t smem, cudaStream_t stream) {
     auto kern = trace_pack_kernel<LOGN>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return check_cuda(cudaGetLastError(), "trace kernel attribute");
+    TFHE_TRY(smem_attr_once((const void*)kern, smem));
     count_launch();
     kern<<<(unsigned)R, 256, smem, stream>>>(a);
     return check_cuda(cudaGetLastError(), "trace kernel launch");
@@ -551,9 +550,7 @@ int tfhe_linear_extract(const int32_t* weights, const int32_t* bias, int32_t J, 
         return fail(TFHE_ERR_INVALID_ARGUMENT, "linear: null pointer");
     if (S > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "linear: at most 65535 ciphertexts per call");
     const size_t smem = (size_t)N * sizeof(uint32_t) + (size_t)LIN_JT * N * sizeof(int32_t);
-    if (cudaFuncSetAttribute(linear_extract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return check_cuda(cudaGetLastError(), "linear kernel attribute");
+    TFHE_TRY(smem_attr_once((const void*)linear_extract_kernel, smem));
     const dim3 grid((J + LIN_JT - 1) / LIN_JT, (unsigned)S);
     count_launch();
     linear_extract_kernel<<<grid, LIN_NT, smem, (cudaStream_t)stream>>>(weights, bias, J, rlwe, N, out_a, out_b);
@@ -568,9 +565,7 @@ int tfhe_lut_mul_sum(const int32_t* luts, int32_t groups, int32_t per_group, con
     if (!luts || !rlwe || !out) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product: null pointer");
     if (S > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product: at most 65535 sequences per call");
     const size_t smem = 3 * (size_t)N * sizeof(uint32_t);
-    if (cudaFuncSetAttribute(lut_mul_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return check_cuda(cudaGetLastError(), "lut product attribute");
+    TFHE_TRY(smem_attr_once((const void*)lut_mul_sum_kernel, smem));
     const dim3 grid((unsigned)per_group, (unsigned)S);
     count_launch();
     lut_mul_sum_kernel<<<grid, LM_NT, smem, (cudaStream_t)stream>>>(luts, groups, per_group, rlwe, N, out);

@@ -106,6 +106,7 @@ struct KsTcArgs {
     // pipelined kernel reads by TMA); false: digits computed in the kernel
     bool allow_alloc;
 };
+int smem_attr_once(const void* kern, size_t smem);
 size_t ks_tc_smem_bytes(int l);
 int ks_tc_columns();
 int launch_ks_tc(const KsTcArgs& args, cudaStream_t stream);

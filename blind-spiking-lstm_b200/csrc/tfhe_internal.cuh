@@ -19,6 +19,13 @@
 #include <mutex>
 #include <string>
 
+// return a non-OK status from the enclosing function
+#define TFHE_TRY(expr)                          \
+    do {                                        \
+        const int _rc = (expr);                 \
+        if (_rc != TFHE_OK) return _rc;         \
+    } while (0)
+
 namespace tfhe {
 
 // ----------------------------------------------------------------------------

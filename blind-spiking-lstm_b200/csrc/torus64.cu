@@ -806,8 +806,7 @@ int launch_trace(const Trace64Args& a, long long R, cudaStream_t stream) {
     const bool fused = trace_fused_enabled() && fsmem <= (size_t)optin;
     const size_t smem = fused ? fsmem : trace_smem(1 << LOGN, a.l);
     const void* kern = fused ? (const void*)trace64_fused_kernel<LOGN> : (const void*)trace64_kernel<LOGN>;
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "trace (2^64) attribute");
+    TFHE_TRY(smem_attr_once(kern, smem));
     count_launch();
     if (fused) trace64_fused_kernel<LOGN><<<(unsigned)R, TRACE_NT, smem, stream>>>(a);
     else trace64_kernel<LOGN><<<(unsigned)R, TRACE_NT, smem, stream>>>(a);
@@ -905,8 +904,7 @@ int tfhe64_linear_extract(const int32_t* weights, const int64_t* bias, int32_t J
     if (!weights || !bias || !rlwe || !out_a || !out_b) return fail(TFHE_ERR_INVALID_ARGUMENT, "linear64: null pointer");
     if (S > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "linear64: at most 65535 ciphertexts per call");
     const size_t smem = (size_t)N * sizeof(u64) + (size_t)LIN_JT * N * sizeof(int32_t);
-    const cudaError_t e = cudaFuncSetAttribute(linear64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "linear64 attribute");
+    TFHE_TRY(smem_attr_once((const void*)linear64_kernel, smem));
     const dim3 grid((J + LIN_JT - 1) / LIN_JT, (unsigned)S);
     count_launch();
     linear64_kernel<<<grid, LIN_NT, smem, (cudaStream_t)stream>>>(
@@ -923,9 +921,7 @@ int tfhe64_lut_mul_sum(const int64_t* luts, int32_t groups, int32_t per_group, c
     if (!luts || !rlwe || !out) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product64: null pointer");
     if (S > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product64: at most 65535 sequences per call");
     const size_t smem = 3 * (size_t)N * sizeof(u64);
-    const cudaError_t e =
-        cudaFuncSetAttribute(lut_mul_sum64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "lut product64 attribute");
+    TFHE_TRY(smem_attr_once((const void*)lut_mul_sum64_kernel, smem));
     const dim3 grid((unsigned)per_group, (unsigned)S);
     count_launch();
     lut_mul_sum64_kernel<<<grid, LM_NT, smem, (cudaStream_t)stream>>>(
