@@ -376,6 +376,142 @@ __global__ void __launch_bounds__(256) limb_fft64_kernel(const u64* __restrict__
     for (int p = tid; p < H; p += nt) dst[(pi * LIMBS + t) * H + p] = buf[swz(p)];
 }
 
+// ---------------------------------------------------------------- LUT x RLWE by FFT
+// The same sums with small LUTs (the step LUTs of the layer hold 0 / +-1):
+// each ciphertext word is split into four signed 16-bit limbs, each limb
+// polynomial multiplied by the LUT in the folded FP64 Fourier domain and the
+// G products summed there; a limb's result is below G N 2^15 2^8 = 2^36 for
+// |LUT| <= 2^8, so it rounds to the exact integer, and the limbs recombine
+// exactly modulo 2^64.  A CTA whose LUTs exceed 2^8 takes the direct sums of
+// lut_mul_sum64_kernel instead (block-uniform), so the result is exact for
+// any LUT.  One CTA per (group slot k, sequence s), the two output
+// polynomials in turn; shared memory: 9 H complex values.
+constexpr int LF_NT = 512;
+constexpr long long LF_MAX_LUT = 256;
+
+template <int LOGN>
+__global__ void __launch_bounds__(LF_NT) lut_fft64_kernel(const long long* __restrict__ P, int G, int Kp,
+                                                          const u64* __restrict__ ct, const double2* qt,
+                                                          const double2* tw, u64* __restrict__ out) {
+    constexpr int N = 1 << LOGN;
+    constexpr int H = N / 2;
+    constexpr int LOGH = LOGN - 1;
+    constexpr int SL = H >= LF_NT ? H / LF_NT : 1;
+    constexpr double inv_h = 1.0 / H;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* work = reinterpret_cast<double2*>(smem_raw);    // 5 H: LUT, 4 limbs
+    double2* acc = work + 5 * H;                              // 4 H: limb products summed over g
+    __shared__ int big;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int k = blockIdx.x;
+    const long long s = blockIdx.y;
+
+    if (tid == 0) big = 0;
+    __syncthreads();
+    for (int g = 0; g < G; ++g) {
+        const long long* lut = P + ((long long)g * Kp + k) * N;
+        for (int i = tid; i < N; i += nt)
+            if (lut[i] > LF_MAX_LUT || lut[i] < -LF_MAX_LUT) big = 1;
+    }
+    __syncthreads();
+    if (big) {
+        // direct negacyclic sums (lut_mul_sum64_kernel's operations)
+        u64* A = reinterpret_cast<u64*>(smem_raw);
+        u64* Bp = A + N;
+        long long* Ps = reinterpret_cast<long long*>(Bp + N);
+        constexpr int CPT = N / LF_NT > 0 ? N / LF_NT : 1;
+        u64 acc_a[CPT], acc_b[CPT];
+#pragma unroll
+        for (int r = 0; r < CPT; ++r) acc_a[r] = acc_b[r] = 0ULL;
+        for (int g = 0; g < G; ++g) {
+            const u64* src = ct + ((s * G + g) * (long long)Kp + k) * 2 * N;
+            const long long* lut = P + ((long long)g * Kp + k) * N;
+            for (int i = tid; i < N; i += nt) {
+                A[i] = src[i];
+                Bp[i] = src[N + i];
+                Ps[i] = lut[i];
+            }
+            __syncthreads();
+            for (int m = 0; m < N; ++m) {
+                const long long w = Ps[m];
+                if (w == 0) continue;
+#pragma unroll
+                for (int r = 0; r < CPT; ++r) {
+                    const int c = tid + LF_NT * r;
+                    if (c >= N) break;
+                    const int idx = c - m;
+                    const u64 va = idx >= 0 ? A[idx] : 0ULL - A[idx + N];
+                    const u64 vb = idx >= 0 ? Bp[idx] : 0ULL - Bp[idx + N];
+                    acc_a[r] += (u64)w * va;
+                    acc_b[r] += (u64)w * vb;
+                }
+            }
+            __syncthreads();
+        }
+        u64* dst = out + (s * Kp + k) * 2 * (long long)N;
+#pragma unroll
+        for (int r = 0; r < CPT; ++r) {
+            const int c = tid + LF_NT * r;
+            if (c >= N) break;
+            dst[c] = acc_a[r];
+            dst[N + c] = acc_b[r];
+        }
+        return;
+    }
+
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int g = 0; g < G; ++g) {
+            const u64* src = ct + ((s * G + g) * (long long)Kp + k) * 2 * N + pass * N;
+            const long long* lut = P + ((long long)g * Kp + k) * N;
+            // fold + twist of the LUT and of the four limbs of the polynomial
+            for (int i = tid; i < H; i += nt) {
+                const double2 w = qt[i];
+                {
+                    const double lo = (double)lut[i], hi = (double)lut[i + H];
+                    work[swz(i)] = make_double2(fma(w.x, lo, w.y * hi), fma(w.y, lo, -w.x * hi));
+                }
+                const u64 xl = src[i], xh = src[i + H];
+#pragma unroll
+                for (int t = 0; t < LIMBS; ++t) {
+                    const double lo = (double)limb16(xl, t), hi = (double)limb16(xh, t);
+                    work[(size_t)(1 + t) * H + swz(i)] = make_double2(fma(w.x, lo, w.y * hi), fma(w.y, lo, -w.x * hi));
+                }
+            }
+            __syncthreads();
+            fwd<LOGH, 0>(work, 5, tw, tid, nt);
+            for (int p = tid; p < H; p += nt) {
+                const double2 f = work[swz(p)];
+#pragma unroll
+                for (int t = 0; t < LIMBS; ++t) {
+                    const double2 v = c_mul(f, work[(size_t)(1 + t) * H + swz(p)]);
+                    double2& a = acc[(size_t)t * H + swz(p)];
+                    if (g == 0) a = v;
+                    else a = make_double2(a.x + v.x, a.y + v.y);
+                }
+            }
+            __syncthreads();
+        }
+        inv<LOGH, Plan<LOGH>::NS - 1>(acc, LIMBS, tw, tid, nt);
+        u64* dst = out + (s * Kp + k) * 2 * (long long)N + pass * N;
+#pragma unroll
+        for (int sl = 0; sl < SL; ++sl) {
+            const int i = tid + sl * nt;
+            if (i >= H) continue;
+            const double2 w = c_conj(qt[i]);
+            u64 lo = 0ULL, hi = 0ULL;
+#pragma unroll
+            for (int t = 0; t < LIMBS; ++t) {
+                const double2 u = c_mul(w, acc[(size_t)t * H + swz(i)]);
+                lo += (u64)(long long)rint(u.x * inv_h) << (16 * t);
+                hi += (u64)(long long)rint(-u.y * inv_h) << (16 * t);
+            }
+            dst[i] = lo;
+            dst[i + H] = hi;
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------- trace
 struct Trace64Args {
     const u64* lwe_a;          // (R, N)
@@ -913,6 +1049,15 @@ int tfhe64_linear_extract(const int32_t* weights, const int64_t* bias, int32_t J
     return check_cuda(cudaGetLastError(), "linear64 launch");
 }
 
+// LUT products in the Fourier domain (TFHE_B200_LUT_FFT=0: the direct sums)
+static bool lut_fft_enabled() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_LUT_FFT");
+        return !(env && env[0] == '0');
+    }();
+    return on;
+}
+
 int tfhe64_lut_mul_sum(const int64_t* luts, int32_t groups, int32_t per_group, const uint64_t* rlwe, int64_t S,
                        int32_t N, uint64_t* out, void* stream) {
     if (!valid_degree(N)) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product64: N must be a power of two");
@@ -920,6 +1065,32 @@ int tfhe64_lut_mul_sum(const int64_t* luts, int32_t groups, int32_t per_group, c
     if (per_group == 0 || S == 0) return TFHE_OK;
     if (!luts || !rlwe || !out) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product64: null pointer");
     if (S > 65535) return fail(TFHE_ERR_INVALID_ARGUMENT, "lut product64: at most 65535 sequences per call");
+    if (lut_fft_enabled() && N <= 2048) {
+        const FftPlan* pl = get_plan(N);
+        if (!pl) return TFHE_ERR_INTERNAL;
+        const size_t fsmem = (size_t)9 * (N / 2) * sizeof(double2);
+        const int logn = log2_exact(N);
+        const void* kern = logn == 7   ? (const void*)lut_fft64_kernel<7>
+                           : logn == 8  ? (const void*)lut_fft64_kernel<8>
+                           : logn == 9  ? (const void*)lut_fft64_kernel<9>
+                           : logn == 10 ? (const void*)lut_fft64_kernel<10>
+                                        : (const void*)lut_fft64_kernel<11>;
+        TFHE_TRY(smem_attr_once(kern, fsmem));
+        const dim3 grid((unsigned)per_group, (unsigned)S);
+        const long long* P = reinterpret_cast<const long long*>(luts);
+        const u64* ct = reinterpret_cast<const u64*>(rlwe);
+        u64* o = reinterpret_cast<u64*>(out);
+        cudaStream_t st = (cudaStream_t)stream;
+        count_launch();
+        switch (logn) {
+            case 7: lut_fft64_kernel<7><<<grid, LF_NT, fsmem, st>>>(P, groups, per_group, ct, pl->qt, pl->tw, o); break;
+            case 8: lut_fft64_kernel<8><<<grid, LF_NT, fsmem, st>>>(P, groups, per_group, ct, pl->qt, pl->tw, o); break;
+            case 9: lut_fft64_kernel<9><<<grid, LF_NT, fsmem, st>>>(P, groups, per_group, ct, pl->qt, pl->tw, o); break;
+            case 10: lut_fft64_kernel<10><<<grid, LF_NT, fsmem, st>>>(P, groups, per_group, ct, pl->qt, pl->tw, o); break;
+            default: lut_fft64_kernel<11><<<grid, LF_NT, fsmem, st>>>(P, groups, per_group, ct, pl->qt, pl->tw, o); break;
+        }
+        return check_cuda(cudaGetLastError(), "lut product64 (FFT) launch");
+    }
     const size_t smem = 3 * (size_t)N * sizeof(u64);
     TFHE_TRY(smem_attr_once((const void*)lut_mul_sum64_kernel, smem));
     const dim3 grid((unsigned)per_group, (unsigned)S);

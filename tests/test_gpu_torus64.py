@@ -173,6 +173,25 @@ def test_cluster_pair_kernel_matches_one_cta_kernel64():
         assert torch.equal(acc, acc1), (B, n_lut)
 
 
+@pytest.mark.parametrize("N,bound,density", [(2048, 1, 0.5), (2048, 256, 1.0), (1024, 255, 0.3), (256, 3, 0.9),
+                                             (2048, 257, 0.2)])
+def test_lut_products_in_the_fourier_domain_are_exact64(N, bound, density):
+    """tfhe64_lut_mul_sum multiplies LUTs with |entries| <= 2^8 in the
+    Fourier domain (16-bit limbs of the ciphertext words) and larger ones by
+    direct sums: exact modulo 2^64 either way, including dense LUTs at the
+    2^8 bound and one entry past it."""
+    rng = np.random.default_rng(N + bound)
+    G, K, S = 4, 5, 2
+    luts = rng.integers(-bound, bound + 1, size=(G, K, N)) * (rng.random((G, K, N)) < density)
+    luts[:, :, 0] = bound                             # the extreme value in every LUT
+    rl = rnd(rng, S, G, K, 2, N)
+    rl[0, 0, 0, 0, :4] = [0, 1 << 63, (1 << 64) - 1, 1 << 32]
+    got = D64.lut_mul_sum(torch.from_numpy(luts).cuda(), d64(rl))
+    for s in range(S):
+        pa, pb = T64.lut_mul_sum(luts, rl[s, :, :, 0], rl[s, :, :, 1])
+        assert np.array_equal(h64(got[s, :, 0]), pa) and np.array_equal(h64(got[s, :, 1]), pb)
+
+
 def test_tensor_memory_kernel_matches_two_per_cta64():
     """The tensor-memory kernel (three ciphertexts per CTA) on the 64-bit
     torus at the reference's parameters: bit-identical to two per CTA."""
