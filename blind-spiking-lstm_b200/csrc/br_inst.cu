@@ -1,5 +1,6 @@
 // Instantiations of the FP64 blind-rotation kernel for one degree.
 // Compiled once per BR_LOGN (7 .. 12) so the degrees build in parallel.
+#include "br_quad.cuh"
 #include "br_split.cuh"
 #include "br_tm.cuh"
 #include "tfhe_dispatch.h"
@@ -65,6 +66,17 @@ BrKernel TFHE_CAT(br_split_logn_, BR_LOGN)(int L) {
         default: return nullptr;
     }
 }
+
+#if BR_LOGN == 10 || BR_LOGN == 11
+BrKernel TFHE_CAT(br_quad32_logn, BR_LOGN)(int L) {
+    switch (L) {
+        case 1: return br_quad_kernel<BR_LOGN, 1, false>;
+        case 2: return br_quad_kernel<BR_LOGN, 2, false>;
+        case 3: return br_quad_kernel<BR_LOGN, 3, false>;
+        default: return nullptr;
+    }
+}
+#endif
 
 #if BR_LOGN == 11
 BrKernel br_tm32_logn11(int L) {

@@ -386,13 +386,11 @@ static bool split_enabled() {
     return on;
 }
 
-static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, const tfhe_tuning* tune) {
-    const bool t64 = args.lwe_a64 != nullptr;
-    BrKernel kern = br_split_kernel_for(ilog2(N), L, t64);
-    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
-    const size_t smem = br_split_smem(N, L, args.G, args.M, br_table_bytes(N));
+// one ciphertext per cluster of `csize` CTAs: grid csize * B
+static int launch_cluster(BrKernel kern, int nt, size_t smem, int csize, const BrArgs& args, int N,
+                          cudaStream_t stream, const tfhe_tuning* tune, const char* what) {
     int per_sm = 1;
-    TFHE_TRY(prepare_kernel((const void*)kern, BR_SPLIT_THREADS, smem, &per_sm));
+    TFHE_TRY(prepare_kernel((const void*)kern, nt, smem, &per_sm));
     BrArgs a = args;
     const FftPlan* pl = get_plan(N);
     if (!pl) return TFHE_ERR_INTERNAL;
@@ -403,27 +401,42 @@ static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, c
     a.K = 1;
     a.l2_prefetch = (tune && tune->l2_prefetch == 0) ? 0 : 1;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(2 * args.B), 1, 1);
-    cfg.blockDim = dim3(BR_SPLIT_THREADS, 1, 1);
+    cfg.gridDim = dim3((unsigned)(csize * args.B), 1, 1);
+    cfg.blockDim = dim3(nt, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.x = csize;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     count_launch();
-    return check_cuda(cudaLaunchKernelEx(&cfg, kern, a), "blind rotation launch (cluster pair)");
+    return check_cuda(cudaLaunchKernelEx(&cfg, kern, a), what);
 }
 
-// clusters of two that can be resident at once (a GPC with an odd number of
-// free SMs leaves one out), cached per device and kernel shape
-static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
+static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, const tfhe_tuning* tune) {
+    const bool t64 = args.lwe_a64 != nullptr;
     BrKernel kern = br_split_kernel_for(ilog2(N), L, t64);
+    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
+    return launch_cluster(kern, BR_SPLIT_THREADS, br_split_smem(N, L, args.G, args.M, br_table_bytes(N)), 2, args, N,
+                          stream, tune, "blind rotation launch (cluster pair)");
+}
+
+static int launch_quad(const BrArgs& args, int N, int L, cudaStream_t stream, const tfhe_tuning* tune) {
+    const bool t64 = args.lwe_a64 != nullptr;
+    BrKernel kern = br_quad_kernel_for(ilog2(N), L, t64);
+    if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
+    return launch_cluster(kern, BR_QUAD_THREADS, br_quad_smem(N, L, args.G, args.M, br_table_bytes(N)), 4, args, N,
+                          stream, tune, "blind rotation launch (cluster of four)");
+}
+
+// clusters of `csize` CTAs of this kernel that can be resident at once (a
+// GPC whose free SMs are not a multiple of the cluster size leaves some out),
+// cached per device, kernel and shape
+static long long resident_clusters(BrKernel kern, int nt, size_t smem, int csize) {
     if (!kern) return 0;
-    const size_t smem = br_split_smem(N, L, G, M, br_table_bytes(N));
     if (smem > (size_t)max_smem_optin()) return 0;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
@@ -436,12 +449,12 @@ static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
     long long n = 0;
     if (cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(2 * std::max(1, sm_count())), 1, 1);
-        cfg.blockDim = dim3(BR_SPLIT_THREADS, 1, 1);
+        cfg.gridDim = dim3((unsigned)(csize * std::max(1, sm_count())), 1, 1);
+        cfg.blockDim = dim3(nt, 1, 1);
         cfg.dynamicSmemBytes = smem;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.x = csize;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
@@ -452,6 +465,34 @@ static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
     cudaGetLastError();   // a refused query only disables the cluster form
     cache.emplace(key, n);
     return n;
+}
+
+static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
+    return resident_clusters(br_split_kernel_for(ilog2(N), L, t64), BR_SPLIT_THREADS,
+                             br_split_smem(N, L, G, M, br_table_bytes(N)), 2);
+}
+
+// One ciphertext per cluster of four CTAs (br_quad.cuh) at N = 1024 and 2048
+// for batches that fit one wave of such clusters: half the pair's per-SM key
+// traffic in the pointwise stage.  TFHE_B200_QUAD=0 turns it off (the pair
+// then takes those batches).
+static bool quad_enabled() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_QUAD");
+        return !(env && env[0] == '0');
+    }();
+    return on;
+}
+
+static bool quad_applies(int N, int L, int G, int M, long long B, bool reflayout, int kr, const tfhe_tuning* tune,
+                         bool t64) {
+    const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
+    if (kr != 0 || reflayout || requested || L > 3 || M > BR_QUAD_MAX_M || M < 2 || !quad_enabled() ||
+        !split_enabled() || B < 1 || 4 * B > sm_count())
+        return false;
+    BrKernel kern = br_quad_kernel_for(ilog2(N), L, t64);
+    if (!kern) return false;
+    return B <= resident_clusters(kern, BR_QUAD_THREADS, br_quad_smem(N, L, G, M, br_table_bytes(N)), 4);
 }
 
 static bool split_applies(int N, int L, int G, int M, long long B, bool reflayout, int kr,
@@ -522,6 +563,8 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
                      int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
     const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
+    if (quad_applies(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
+        return launch_quad(args, N, L, stream, tune);
     if (split_applies(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
         return launch_split(args, N, L, stream, tune);
     if (!reflayout && kr == 0 && N == 2048 && L <= 2 &&
@@ -1399,9 +1442,9 @@ int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* cipher
 int32_t tfhe_keys_cluster_size(const tfhe_keys* keys, int64_t batch) {
     if (!keys) return 0;
     const tfhe_params& p = keys->p;
-    return split_applies(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, p.log2_q == 64)
-               ? 2
-               : 1;
+    const bool t64 = p.log2_q == 64;
+    if (quad_applies(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, t64)) return 4;
+    return split_applies(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, t64) ? 2 : 1;
 }
 
 int64_t tfhe_launch_count(void) { return launch_count(); }

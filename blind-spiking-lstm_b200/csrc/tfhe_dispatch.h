@@ -2,6 +2,7 @@
 // the FP64 blind-rotation kernels and the key-FFT kernel of its degree.
 #pragma once
 
+#include "br_quad.cuh"
 #include "br_split.cuh"
 #include "br_tm.cuh"
 
@@ -62,6 +63,17 @@ inline BrKernel br_split_kernel_for(int logn, int L, bool t64) {
         case 12: return t64 ? br_split64_logn_12(L) : br_split_logn_12(L);
         default: return nullptr;
     }
+}
+
+// the cluster-of-four kernels of small batches, N = 1024 and 2048
+BrKernel br_quad32_logn10(int L);
+BrKernel br_quad32_logn11(int L);
+BrKernel br_quad64_logn10(int L);
+BrKernel br_quad64_logn11(int L);
+inline BrKernel br_quad_kernel_for(int logn, int L, bool t64) {
+    if (logn == 10) return t64 ? br_quad64_logn10(L) : br_quad32_logn10(L);
+    if (logn == 11) return t64 ? br_quad64_logn11(L) : br_quad32_logn11(L);
+    return nullptr;
 }
 
 // the tensor-memory kernels (three ciphertexts per CTA), N = 2048 only

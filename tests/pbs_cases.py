@@ -21,9 +21,17 @@ PARAMS = {
                     sigma_glwe=2.0 ** 6, sigma_lwe=2.0 ** 16),
     "c4_N4096": dict(q=Q, N=4096, n=8, beta_bs=2 ** 10, l_bs=1, collapse=4, beta_ks=2 ** 4, l_ks=4,
                      sigma_glwe=1.0, sigma_lwe=2.0 ** 15),
+    # the cluster-of-four kernel's other level counts: one level (the CTAs of
+    # odd rank transform nothing) and three (two levels on the even ranks)
+    "c1_N1024_l1": dict(q=Q, N=1024, n=12, beta_bs=2 ** 10, l_bs=1, collapse=1, beta_ks=2 ** 4, l_ks=4,
+                        sigma_glwe=1.0, sigma_lwe=2.0 ** 15),
+    "c3_N2048_l3": dict(q=Q, N=2048, n=18, beta_bs=2 ** 7, l_bs=3, collapse=3, beta_ks=2 ** 3, l_ks=5,
+                        sigma_glwe=2.0 ** 7, sigma_lwe=2.0 ** 17),
 }
-KEY_SEED = {"tiny_c3": 11, "tiny_c2": 12, "cfg1": 13, "cfg2": 14, "c1_N128": 15, "c4_N4096": 16}
-INPUT_SEED = {"tiny_c3": 21, "tiny_c2": 22, "cfg1": 23, "cfg2": 24, "c1_N128": 25, "c4_N4096": 26}
+KEY_SEED = {"tiny_c3": 11, "tiny_c2": 12, "cfg1": 13, "cfg2": 14, "c1_N128": 15, "c4_N4096": 16, "c1_N1024_l1": 17,
+            "c3_N2048_l3": 18}
+INPUT_SEED = {"tiny_c3": 21, "tiny_c2": 22, "cfg1": 23, "cfg2": 24, "c1_N128": 25, "c4_N4096": 26, "c1_N1024_l1": 27,
+              "c3_N2048_l3": 28}
 
 
 def canon(x):

@@ -518,23 +518,38 @@ def test_keyswitch_unaligned_input_uses_cuda_cores():
     assert np.array_equal(host_u32(ga), u32(ra)) and np.array_equal(host_u32(gb), u32(rb.reshape(-1)))
 
 
-@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2", "c1_N128", "c4_N4096"])
-def test_cluster_pair_kernel_matches_one_cta_kernel(name):
-    """Small batches run one ciphertext on a cluster of two CTAs (each owns
-    one ACC polynomial); the outputs are bit-identical to the one-CTA
-    kernel's (requested shape K = 1), at every parameter set, for the
-    extraction (n_lut 1 and 4) and for the rotated accumulator."""
+def quad_form(name):
+    """whether small batches of this set run on clusters of four CTAs"""
+    p = PARAMS[name]
+    return p["N"] in (1024, 2048) and p["l_bs"] <= 3 and 2 ** p["collapse"] <= 8
+
+
+@pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2", "c1_N128", "c4_N4096", "c1_N1024_l1",
+                                  "c3_N2048_l3"])
+def test_cluster_kernels_match_one_cta_kernel(name):
+    """Small batches run one ciphertext on a cluster of four CTAs (N = 1024
+    and 2048, collapse <= 3: each CTA owns one ACC polynomial and half of the
+    spectrum) or of two (each owns one ACC polynomial); the outputs are
+    bit-identical to the one-CTA kernel's (requested shape K = 1), at every
+    parameter set, for the extraction (n_lut 1 and 4) and for the rotated
+    accumulator."""
     p = PARAMS[name]
     N = p["N"]
     eng = engine(name)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    for batch, n_lut in ((1, 1), (5, 4), (sms // 2, 1)):
+    for batch, n_lut in ((1, 1), (5, 4), (sms // 4, 1), (sms // 2, 1)):
         msgs, a, b = inputs(name, batch, seed_offset=batch)
         body = step_body(name) if n_lut == 1 else many_lut_body(name, n_lut)
         lut = device_u32(np.stack([np.zeros(N), body])[None])
         a_d, b_d = device_u32(a), device_u32(b.reshape(-1))
         eng.set_tuning()
-        assert eng.cluster_size(batch) == 2
+        cs = eng.cluster_size(batch)
+        if batch <= 5:
+            assert cs == (4 if quad_form(name) else 2), (batch, cs)
+        elif batch == sms // 2:
+            assert cs == 2, (batch, cs)
+        else:
+            assert cs in (2, 4), (batch, cs)
         got = eng.pbs(a_d, b_d, lut, n_lut=n_lut)
         ka, kb = eng.keyswitch(a_d, b_d)
         acc = eng.blind_rotate(ka, kb, lut, n_lut=n_lut)
@@ -543,8 +558,8 @@ def test_cluster_pair_kernel_matches_one_cta_kernel(name):
         want = eng.pbs(a_d, b_d, lut, n_lut=n_lut)
         acc1 = eng.blind_rotate(ka, kb, lut, n_lut=n_lut)
         eng.set_tuning()
-        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (batch, n_lut)
-        assert torch.equal(acc, acc1), (batch, n_lut)
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (batch, n_lut, cs)
+        assert torch.equal(acc, acc1), (batch, n_lut, cs)
     assert eng.cluster_size(sms // 2 + 1) == 1
 
 

@@ -151,17 +151,24 @@ def test_native_and_reference_layout_chains_agree64():
     assert d.max() <= 2.0 ** 50
 
 
-def test_cluster_pair_kernel_matches_one_cta_kernel64():
-    """Small batches on cluster pairs give the one-CTA kernel's outputs bit
-    for bit on the 64-bit torus (reference parameters, n_lut 1 and 4)."""
+def test_cluster_kernels_match_one_cta_kernel64():
+    """Small batches on clusters of four CTAs (up to a quarter of the SM
+    count) and of two give the one-CTA kernel's outputs bit for bit on the
+    64-bit torus (reference parameters, n_lut 1 and 4)."""
     p = C64.REF64
     ck, dk, ok = keys_for(p)
     rng = np.random.default_rng(45)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    for B, n_lut in ((1, 1), (6, 4), (sms // 2, 1)):
+    for B, n_lut in ((1, 1), (6, 4), (sms // 4, 1), (sms // 2, 1)):
         lut_d, a_d, b_d = d64(rnd(rng, B, 2, p.N)), d64(rnd(rng, B, p.n)), d64(rnd(rng, B))
         dk.set_tuning()
-        assert dk.cluster_size(B) == 2
+        cs = dk.cluster_size(B)
+        if B <= 6:
+            assert cs == 4, (B, cs)
+        elif B == sms // 2:
+            assert cs == 2, (B, cs)
+        else:
+            assert cs in (2, 4), (B, cs)
         got = dk.cuboot_merge(a_d, b_d, lut_d, n_lut)
         acc = dk.blind_rotate(a_d, b_d, lut_d, n_lut)
         dk.set_tuning(ciphertexts_per_cta=1)
@@ -169,8 +176,8 @@ def test_cluster_pair_kernel_matches_one_cta_kernel64():
         want = dk.cuboot_merge(a_d, b_d, lut_d, n_lut)
         acc1 = dk.blind_rotate(a_d, b_d, lut_d, n_lut)
         dk.set_tuning()
-        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (B, n_lut)
-        assert torch.equal(acc, acc1), (B, n_lut)
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (B, n_lut, cs)
+        assert torch.equal(acc, acc1), (B, n_lut, cs)
 
 
 @pytest.mark.parametrize("N,bound,density", [(2048, 1, 0.5), (2048, 256, 1.0), (1024, 255, 0.3), (256, 3, 0.9),
