@@ -183,45 +183,68 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
             }
             const int* rot = rot_all + (size_t)g * M;
 
-            // prologue: the digit levels lvl = h + 2 s of polynomial r, each
-            // from the digit chain run up to it (the chain's operations, so
-            // the same digits), fold + twist, first DIF superstage
+            // prologue: the digit levels lvl = h, h + 2, ... of polynomial r,
+            // fold + twist, first DIF superstage
             if (owner) {
                 double2 w0[8];
                 w0[0] = make_double2(1.0, 0.0);
 #pragma unroll
                 for (int k2 = 1; k2 < 8; ++k2) w0[k2] = tw[(k2 - 1) * Q8 + on1];
-                auto level = [&](int sl) {
-                    const int lvl = h + 2 * sl;
-                    double2 v[8];
-#pragma unroll
-                    for (int n2 = 0; n2 < 8; ++n2) {
-                        double ylo = acc_lo[n2] * inv_qb;
-                        double dlo = rint(ylo);
-                        double yhi = acc_hi[n2] * inv_qb;
-                        double dhi = rint(yhi);
-                        for (int l2 = 1; l2 <= lvl; ++l2) {
-                            ylo = (ylo - dlo) * beta;
-                            dlo = rint(ylo);
-                            yhi = (yhi - dhi) * beta;
-                            dhi = rint(yhi);
-                        }
-                        const double2 w = qtab(on1 + Q8 * n2);
-                        v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
-                    }
-                    dft8<false>(v);
-#pragma unroll
-                    for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
-                    double2* poly = spec + sl * H;
-#pragma unroll
-                    for (int k2 = 0; k2 < 8; ++k2) poly[swz(on1 + Q8 * k2)] = v[k2];
-                };
-                // (a loop with a constant trip count where there is one own
-                // level at most: fewer live registers)
                 if constexpr (LH == 1) {
-                    if (nown > 0) level(0);
+                    // l_bs <= 2: one own level at most, its digits from the
+                    // chain run up to it (the chain's operations, so the same
+                    // digits); one straight-line body keeps the registers low
+                    if (nown > 0) {
+                        double2 v[8];
+#pragma unroll
+                        for (int n2 = 0; n2 < 8; ++n2) {
+                            double ylo = acc_lo[n2] * inv_qb;
+                            double dlo = rint(ylo);
+                            double yhi = acc_hi[n2] * inv_qb;
+                            double dhi = rint(yhi);
+                            if (h == 1) {
+                                ylo = (ylo - dlo) * beta;
+                                dlo = rint(ylo);
+                                yhi = (yhi - dhi) * beta;
+                                dhi = rint(yhi);
+                            }
+                            const double2 w = qtab(on1 + Q8 * n2);
+                            v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
+                        }
+                        dft8<false>(v);
+#pragma unroll
+                        for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
+#pragma unroll
+                        for (int k2 = 0; k2 < 8; ++k2) spec[swz(on1 + Q8 * k2)] = v[k2];
+                    }
                 } else {
-                    for (int sl = 0; sl < nown; ++sl) level(sl);
+                    // l_bs = 3: every level's digits and transform (the chain
+                    // runs through all of them), stored for the own levels only,
+                    // so both halves run one instruction stream
+                    double x_lo[8], x_hi[8];
+#pragma unroll
+                    for (int lvl = 0; lvl < L; ++lvl) {
+                        double2 v[8];
+#pragma unroll
+                        for (int n2 = 0; n2 < 8; ++n2) {
+                            const double ylo = lvl == 0 ? acc_lo[n2] * inv_qb : x_lo[n2] * beta;
+                            const double dlo = rint(ylo);
+                            x_lo[n2] = ylo - dlo;
+                            const double yhi = lvl == 0 ? acc_hi[n2] * inv_qb : x_hi[n2] * beta;
+                            const double dhi = rint(yhi);
+                            x_hi[n2] = yhi - dhi;
+                            const double2 w = qtab(on1 + Q8 * n2);
+                            v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
+                        }
+                        dft8<false>(v);
+#pragma unroll
+                        for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
+                        double2* poly = spec + (lvl >> 1) * H;
+                        const bool own_level = (lvl & 1) == h;
+#pragma unroll
+                        for (int k2 = 0; k2 < 8; ++k2)
+                            if (own_level) poly[swz(on1 + Q8 * k2)] = v[k2];
+                    }
                 }
             }
             __syncthreads();
