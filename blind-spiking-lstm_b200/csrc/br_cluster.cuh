@@ -1,90 +1,95 @@
-// Small-batch blind rotation: one ciphertext per cluster of four CTAs.
+// Small-batch blind rotation: one ciphertext per cluster of 2 S CTAs
+// (S = 2: four CTAs, S = 4: eight).
 //
 // At batch 1 the cluster-pair kernel (br_split.cuh) spends about half of each
 // group in the pointwise stage (n=742 N=2048: 8.8k of 16.6k cycles; n=630
 // N=1024 with eight patterns: 12.0k of 18.9k), pulling output r's half of the
-// group's key into one SM.  Here CTA (r, h) (cluster rank r + 2 h) owns ACC
-// polynomial r and half h of the spectrum's positions:
+// group's key into one SM.  Here CTA (r, h) (cluster rank r + 2 h, h < S) owns
+// ACC polynomial r and part h of the S parts of the spectrum's positions:
 //   * the prologue transforms the gadget digits of polynomial r at the levels
-//     lvl with lvl % 2 == h (one forward FFT at l_bs = 2 instead of two);
+//     lvl with lvl % S == h (one forward FFT at most where l_bs <= S);
 //   * after a cluster barrier, the pointwise stage computes output r at the
-//     positions of half h, from the four CTAs' digit spectra (distributed
-//     shared memory) and the key words of those positions only: a quarter of
+//     positions of part h, from the cluster's digit spectra (distributed
+//     shared memory) and the key words of those positions only: 1 / (2 S) of
 //     the group's key per SM;
-//   * the inverse superstages but the last stay inside a half (their
-//     butterfly groups span at most H/8 positions); after a second cluster
-//     barrier both CTAs of polynomial r run the last superstage over both
-//     halves (half of its reads from the partner), so each holds the whole
-//     next ACC polynomial r for its next prologue.
-// At N = 1024 a half holds 256 positions for 512 threads: two adjacent lanes
-// share a position, lane 0 contracting the first M/2 patterns and lane 1 the
-// others, and lane 1 continues lane 0's sum after one shuffle, so the sum over
-// patterns keeps its order.  Every value is computed by the same operations in
-// the same order as br_fp64_kernel (digits, FFT stages, the key contraction in
-// digit order per pattern, the twist products in pattern order, the
-// rounding), so the outputs are bit-identical to it.
+//   * the inverse superstages but the last stay inside a part (their
+//     butterfly groups span at most H/8 positions, a part at least H/4);
+//     after a second cluster barrier the S CTAs of polynomial r each run the
+//     last superstage over all parts (8/S of its 8 points per part), so each
+//     holds the whole next ACC polynomial r for its next prologue.
+// Where a part holds half as many positions as the CTA has threads, two
+// adjacent lanes share a position, lane 0 contracting the first M/2 patterns
+// and lane 1 the others, and lane 1 continues lane 0's sum after one shuffle,
+// so the sum over patterns keeps its order.  Every value is computed by the
+// same operations in the same order as br_fp64_kernel (digits, FFT stages,
+// the key contraction in digit order per pattern, the twist products in
+// pattern order, the rounding), so the outputs are bit-identical to it.
 //
 // Shared memory is single-buffered.  CTA (r, h) rewrites its digit spectra in
 // group g + 1 only after the second barrier of group g, which every CTA
-// reaches after its pointwise reads of group g; it rewrites its output half in
-// group g + 1 only after the first barrier of group g + 1, which the partner
-// reaches after its last-superstage reads of group g.  A barrier after each
-// ciphertext's last group keeps the output halves alive for those reads before
-// the epilogue reuses them, and a last one keeps each CTA's shared memory until
-// no peer reads it.  Every thread of the four CTAs reaches the same barriers
-// the same number of times (loop bounds depend only on the cluster index).
+// reaches after its pointwise reads of group g; it rewrites its output part in
+// group g + 1 only after the first barrier of group g + 1, which the other CTAs
+// of polynomial r reach after their last-superstage reads of group g.  A
+// barrier after each ciphertext's last group keeps the output parts alive for
+// those reads before the epilogue reuses them, and a last one keeps each CTA's
+// shared memory until no peer reads it.  Every thread of the cluster reaches
+// the same barriers the same number of times (loop bounds depend only on the
+// cluster index).
 #pragma once
 
 #include "br_split.cuh"
 
 namespace tfhe {
 
-constexpr int BR_QUAD_THREADS = 512;
-constexpr int BR_QUAD_MAX_M = 8;      // patterns (collapse <= 3)
+constexpr int BR_CLUSTER_THREADS = 512;
+constexpr int BR_CLUSTER_MAX_M = 8;   // patterns (collapse <= 3)
 
-// shared memory of br_quad_kernel: the own digit levels [ceil(L/2)][H], the
-// output polynomial [H] (half h used), the tables, the rotation indices of
-// every group and b~
-inline size_t br_quad_smem(int N, int L, int G, int M, size_t table_bytes) {
+// shared memory of br_cluster_kernel: the own digit levels [ceil(L/S)][H],
+// the output polynomial [H] (part h used), the tables, the rotation indices
+// of every group and b~
+inline size_t br_cluster_smem(int N, int L, int G, int M, size_t table_bytes, int S) {
     const int H = N / 2;
-    const int LH = (L + 1) / 2;
+    const int LH = (L + S - 1) / S;
     return (size_t)(LH + 1) * H * sizeof(double2) + table_bytes + ((size_t)G * M + 1) * sizeof(int) + 16;
 }
 
-// inverse superstages s = S0 .. 1 over the butterflies of half h of one
-// polynomial (their groups of R * S <= H / 8 positions lie inside a half)
-template <int LOGH, int s>
-__device__ __forceinline__ void inverse_middle_half(double2* poly, int h, const double2* tw, int tid, int nt) {
+// inverse superstages s = S0 .. 1 over the butterflies of part h of the
+// NP parts of one polynomial (their groups of R * span <= H / 8 positions lie
+// inside a part of H / NP >= H / 4)
+template <int LOGH, int s, int NP>
+__device__ __forceinline__ void inverse_middle_part(double2* poly, int h, const double2* tw, int tid, int nt) {
     if constexpr (s >= 1) {
         using PL = Plan<LOGH>;
         constexpr int R = PL::radix(s);
-        constexpr int S = PL::span(s);
-        constexpr int PERH = PL::H / R / 2;
-        static_assert(PERH % S == 0, "whole butterfly groups per half");
+        constexpr int SP = PL::span(s);
+        constexpr int PERP = PL::H / R / NP;
+        static_assert(PERP % SP == 0, "whole butterfly groups per part");
         const double2* tws = tw + PL::tw_offset(s);
-        for (int t = tid; t < PERH; t += nt) dit_stage<R, S>(poly, tws, h * PERH + t);
+        for (int t = tid; t < PERP; t += nt) dit_stage<R, SP>(poly, tws, h * PERP + t);
         __syncthreads();
-        inverse_middle_half<LOGH, s - 1>(poly, h, tw, tid, nt);
+        inverse_middle_part<LOGH, s - 1, NP>(poly, h, tw, tid, nt);
     }
 }
 
-template <int LOGN, int L, bool T64>
-__global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArgs args) {
+template <int LOGN, int L, bool T64, int S>
+__global__ void __launch_bounds__(BR_CLUSTER_THREADS, 1) br_cluster_kernel(const BrArgs args) {
     constexpr int N = 1 << LOGN;
     constexpr int H = N / 2;
     constexpr int LOGH = LOGN - 1;
     constexpr int P = 2 * L;
     constexpr int Q8 = H / 8;
-    constexpr int LH = (L + 1) / 2;
-    constexpr int HALF = H / 2;
-    constexpr int TPS = BR_QUAD_THREADS / HALF;          // lanes per position in the pointwise stage
+    constexpr int LH = (L + S - 1) / S;                  // own digit levels at most
+    constexpr int PART = H / S;                          // positions per part
+    constexpr int PPP = 8 / S;                           // last-superstage points per part
+    constexpr int TPS = BR_CLUSTER_THREADS / PART;       // lanes per position in the pointwise stage
     using PL = Plan<LOGH>;
-    static_assert(TPS == 1 || TPS == 2, "N = 1024 or 2048");
-    static_assert(Q8 * 4 == HALF, "the last superstage reads four points of each half");
+    static_assert(S == 2 || S == 4, "clusters of four or eight CTAs");
+    static_assert(TPS == 1 || TPS == 2, "one or two lanes per position");
+    static_assert(Q8 * PPP == PART, "the last superstage reads 8/S points of each part");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int M = args.M;
-    double2* spec = reinterpret_cast<double2*>(smem_raw);   // [LH][H]: levels h, h + 2, ...
+    double2* spec = reinterpret_cast<double2*>(smem_raw);   // [LH][H]: levels h, h + S, ...
     double2* outp = spec + LH * H;                           // [H]
     double2* qt_s = outp + H;                                // N / 2, swizzled
     double2* tw = qt_s + N / 2;                              // PL::TW
@@ -97,7 +102,7 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
     const int nt = blockDim.x;
     const int rank = (int)cluster_rank();
     const int r = rank & 1;                                  // ACC polynomial / output
-    const int h = rank >> 1;                                 // half of the positions, parity of the levels
+    const int h = rank >> 1;                                 // part of the positions, levels mod S
     const long long cl = cluster_index_x();
     const long long ncl = cluster_count_x();
     const long long mine = cl < args.B ? (args.B - cl + ncl - 1) / ncl : 0;
@@ -106,15 +111,17 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
     for (int i = tid; i < N / 2; i += nt) qt_s[qsw<LOGN>(i)] = args.qt[i];
     for (int i = tid; i < PL::TW; i += nt) tw[i] = args.tw[i];
     for (int i = tid; i < H; i += nt) freq[i] = args.freq[i];
-    uint32_t spec_of[4];                                     // digit spectra of each rank
+    uint32_t spec_of[2 * S];                                 // digit spectra of each rank
 #pragma unroll
-    for (int k = 0; k < 4; ++k) spec_of[k] = peer_smem(spec, (uint32_t)k);
-    const uint32_t partner_out = peer_smem(outp, (uint32_t)(rank ^ 2));
+    for (int k = 0; k < 2 * S; ++k) spec_of[k] = peer_smem(spec, (uint32_t)k);
+    uint32_t out_of[S];                                      // output parts of polynomial r
+#pragma unroll
+    for (int k = 0; k < S; ++k) out_of[k] = peer_smem(outp, (uint32_t)(r + 2 * k));
     cluster_barrier();                                       // every CTA of the cluster has started
 
     const bool owner = tid < Q8;
     const int on1 = tid;
-    const int nown = (L - h + 1) / 2;                        // own digit levels
+    const int nown = h < L ? (L - 1 - h) / S + 1 : 0;        // own digit levels
     const double q = ldexp(1.0, args.log2_q);
     const double inv_q = ldexp(1.0, -args.log2_q);
     const double beta = ldexp(1.0, args.log2_beta);
@@ -169,7 +176,7 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
         }
 
         for (int g = 0; g < args.G; ++g) {
-            // the next group's key words of (output r, half h) into L2: one
+            // the next group's key words of (output r, part h) into L2: one
             // region (digit pair, pattern) per cluster in turn
             if (g + 1 < args.G && args.l2_prefetch) {
                 const int regions = (P / 2) * M;
@@ -177,13 +184,13 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                     if (i % ncl32 == cl32) {
                         const double2* base = args.bsk + (size_t)(g + 1) * 2 * P * M * H +
                                               (size_t)r * (P / 2) * M * H * 2 + (size_t)i * H * 2 +
-                                              (size_t)h * HALF * 2;
-                        prefetch_l2_bulk(base, (uint32_t)(HALF * 2 * sizeof(double2)));
+                                              (size_t)h * PART * 2;
+                        prefetch_l2_bulk(base, (uint32_t)(PART * 2 * sizeof(double2)));
                     }
             }
             const int* rot = rot_all + (size_t)g * M;
 
-            // prologue: the digit levels lvl = h, h + 2, ... of polynomial r,
+            // prologue: the digit levels lvl = h, h + S, ... of polynomial r,
             // fold + twist, first DIF superstage
             if (owner) {
                 double2 w0[8];
@@ -191,9 +198,10 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
 #pragma unroll
                 for (int k2 = 1; k2 < 8; ++k2) w0[k2] = tw[(k2 - 1) * Q8 + on1];
                 if constexpr (LH == 1) {
-                    // l_bs <= 2: one own level at most, its digits from the
-                    // chain run up to it (the chain's operations, so the same
-                    // digits); one straight-line body keeps the registers low
+                    // l_bs <= S: one own level at most (lvl = h), its digits
+                    // from the chain run up to it (the chain's operations, so
+                    // the same digits); one straight-line body keeps the
+                    // registers low
                     if (nown > 0) {
                         double2 v[8];
 #pragma unroll
@@ -202,12 +210,14 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                             double dlo = rint(ylo);
                             double yhi = acc_hi[n2] * inv_qb;
                             double dhi = rint(yhi);
-                            if (h == 1) {
-                                ylo = (ylo - dlo) * beta;
-                                dlo = rint(ylo);
-                                yhi = (yhi - dhi) * beta;
-                                dhi = rint(yhi);
-                            }
+#pragma unroll
+                            for (int l2 = 1; l2 < L; ++l2)
+                                if (l2 <= h) {
+                                    ylo = (ylo - dlo) * beta;
+                                    dlo = rint(ylo);
+                                    yhi = (yhi - dhi) * beta;
+                                    dhi = rint(yhi);
+                                }
                             const double2 w = qtab(on1 + Q8 * n2);
                             v[n2] = make_double2(fma(w.x, dlo, w.y * dhi), fma(w.y, dlo, -w.x * dhi));
                         }
@@ -218,9 +228,9 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                         for (int k2 = 0; k2 < 8; ++k2) spec[swz(on1 + Q8 * k2)] = v[k2];
                     }
                 } else {
-                    // l_bs = 3: every level's digits and transform (the chain
-                    // runs through all of them), stored for the own levels only,
-                    // so both halves run one instruction stream
+                    // l_bs > S: every level's digits and transform (the chain
+                    // runs through all of them), stored for the own levels
+                    // only, so every part runs one instruction stream
                     double x_lo[8], x_hi[8];
 #pragma unroll
                     for (int lvl = 0; lvl < L; ++lvl) {
@@ -239,8 +249,8 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                         dft8<false>(v);
 #pragma unroll
                         for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], w0[k2]);
-                        double2* poly = spec + (lvl >> 1) * H;
-                        const bool own_level = (lvl & 1) == h;
+                        double2* poly = spec + (lvl / S) * H;
+                        const bool own_level = (lvl % S) == h;
 #pragma unroll
                         for (int k2 = 0; k2 < 8; ++k2)
                             if (own_level) poly[swz(on1 + Q8 * k2)] = v[k2];
@@ -251,18 +261,18 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
             forward_middle<LOGH, 1>(spec, nown, tw, tid, nt);
             cluster_barrier();                               // all digit spectra are complete
 
-            // pointwise: output r at the positions of half h,
+            // pointwise: output r at the positions of part h,
             // out = sum_m X^{r_m} * sum_bc BSK[g, r, bc, m] * DEC[bc]
             {
                 const size_t gbase = (size_t)g * 2 * P * M * H;
-                const int p = h * HALF + tid / TPS;
+                const int p = h * PART + tid / TPS;
                 double2 d[P];
 #pragma unroll
                 for (int lvl = 0; lvl < L; ++lvl)
 #pragma unroll
                     for (int in = 0; in < 2; ++in) {
-                        const int src = in + 2 * (lvl & 1);          // rank holding digit (lvl, in)
-                        const int e_off = (lvl >> 1) * H + swz(p);
+                        const int src = in + 2 * (lvl % S);          // rank holding digit (lvl, in)
+                        const int e_off = (lvl / S) * H + swz(p);
                         d[2 * lvl + in] = src == rank ? spec[e_off]
                                                       : ld_peer(spec_of[src] + (uint32_t)(e_off * sizeof(double2)));
                     }
@@ -303,9 +313,9 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                     const int u = tid & 1;
                     const int mlen = M >> 1;
                     const int mbeg = u * mlen;
-                    double2 tt[BR_QUAD_MAX_M / 2];
+                    double2 tt[BR_CLUSTER_MAX_M / 2];
 #pragma unroll
-                    for (int i = 0; i < BR_QUAD_MAX_M / 2; ++i) {
+                    for (int i = 0; i < BR_CLUSTER_MAX_M / 2; ++i) {
                         tt[i] = make_double2(0.0, 0.0);
                         if (i < mlen) {
                             const int m = mbeg + i;
@@ -330,7 +340,7 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                     if (u == 1) {
                         o = prev;
 #pragma unroll
-                        for (int i = 0; i < BR_QUAD_MAX_M / 2; ++i)
+                        for (int i = 0; i < BR_CLUSTER_MAX_M / 2; ++i)
                             if (i < mlen) {
                                 const double2 w = root2n<LOGN, true>(qt_s, rot[mbeg + i] * e);
                                 c_mac(o, w, tt[i]);
@@ -340,17 +350,17 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                 }
             }
             __syncthreads();
-            inverse_middle_half<LOGH, PL::NS - 1>(outp, h, tw, tid, nt);
-            cluster_barrier();                               // both halves of output r are transformed
+            inverse_middle_part<LOGH, PL::NS - 1, S>(outp, h, tw, tid, nt);
+            cluster_barrier();                               // every part of output r is transformed
 
-            // last DIT superstage over both halves, untwist, round, centred
+            // last DIT superstage over all parts, untwist, round, centred
             // reduction: the whole next ACC polynomial r
             if (owner) {
                 double2 v[8];
 #pragma unroll
                 for (int k2 = 0; k2 < 8; ++k2) {
                     const int e_off = swz(on1 + Q8 * k2);
-                    v[k2] = (k2 >> 2) == h ? outp[e_off] : ld_peer(partner_out + (uint32_t)(e_off * sizeof(double2)));
+                    v[k2] = k2 / PPP == h ? outp[e_off] : ld_peer(out_of[k2 / PPP] + (uint32_t)(e_off * sizeof(double2)));
                 }
                 twiddle<8, Q8, true>(v, tw, on1);
                 dft8<true>(v);
@@ -369,10 +379,10 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
                 for (int n2 = 0; n2 < 8; ++n2) acc_lo[n2] = acc_hi[n2] = 0.0;
             }
         }
-        cluster_barrier();                                   // the partner has read this CTA's output half
+        cluster_barrier();                                   // the peers have read this CTA's output part
 
         // epilogue: polynomial r rotated by -b~; the CTAs of polynomial 0
-        // extract the masks, those of polynomial 1 the bodies, each half h
+        // extract the masks, those of polynomial 1 the bodies, each part h
         // of the words
         if constexpr (T64) {
             typedef unsigned long long u64;
@@ -391,11 +401,11 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
             __syncthreads();
             const int bx = bexp[0];
             if (args.acc_out64)
-                for (int i = h * H + tid; i < (h + 1) * H; i += nt)
+                for (int i = h * (N / S) + tid; i < (h + 1) * (N / S); i += nt)
                     args.acc_out64[ct * 2 * N + r * N + i] = ncoef64<LOGN>(acc, i + bx);
             const int nl = args.n_lut;
             if (args.out_a64 && r == 0)
-                for (int t = h * nl * H + tid; t < (h + 1) * nl * H; t += nt) {
+                for (int t = h * nl * (N / S) + tid; t < (h + 1) * nl * (N / S); t += nt) {
                     const int al = t / N;
                     const int jx = t - al * N;
                     args.out_a64[ct * nl * N + t] = ncoef64<LOGN>(acc, al - jx + bx);
@@ -418,11 +428,11 @@ __global__ void __launch_bounds__(BR_QUAD_THREADS, 1) br_quad_kernel(const BrArg
             __syncthreads();
             const int bx = bexp[0];
             if (args.acc_out)
-                for (int i = h * H + tid; i < (h + 1) * H; i += nt)
+                for (int i = h * (N / S) + tid; i < (h + 1) * (N / S); i += nt)
                     args.acc_out[ct * 2 * N + r * N + i] = ncoef<LOGN>(acc, i + bx);
             const int nl = args.n_lut;
             if (args.out_a && r == 0)
-                for (int t = h * nl * H + tid; t < (h + 1) * nl * H; t += nt) {
+                for (int t = h * nl * (N / S) + tid; t < (h + 1) * nl * (N / S); t += nt) {
                     const int al = t / N;
                     const int jx = t - al * N;
                     args.out_a[ct * nl * N + t] = ncoef<LOGN>(acc, al - jx + bx);

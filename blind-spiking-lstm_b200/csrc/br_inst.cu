@@ -1,6 +1,6 @@
 // Instantiations of the FP64 blind-rotation kernel for one degree.
 // Compiled once per BR_LOGN (7 .. 12) so the degrees build in parallel.
-#include "br_quad.cuh"
+#include "br_cluster.cuh"
 #include "br_split.cuh"
 #include "br_tm.cuh"
 #include "tfhe_dispatch.h"
@@ -68,13 +68,26 @@ BrKernel TFHE_CAT(br_split_logn_, BR_LOGN)(int L) {
 }
 
 #if BR_LOGN == 10 || BR_LOGN == 11
-BrKernel TFHE_CAT(br_quad32_logn, BR_LOGN)(int L) {
-    switch (L) {
-        case 1: return br_quad_kernel<BR_LOGN, 1, false>;
-        case 2: return br_quad_kernel<BR_LOGN, 2, false>;
-        case 3: return br_quad_kernel<BR_LOGN, 3, false>;
-        default: return nullptr;
+BrKernel TFHE_CAT(br_cluster32_logn, BR_LOGN)(int L, int S) {
+    if (S == 2) {
+        switch (L) {
+            case 1: return br_cluster_kernel<BR_LOGN, 1, false, 2>;
+            case 2: return br_cluster_kernel<BR_LOGN, 2, false, 2>;
+            case 3: return br_cluster_kernel<BR_LOGN, 3, false, 2>;
+            default: return nullptr;
+        }
     }
+#if BR_LOGN == 11
+    if (S == 4) {
+        switch (L) {
+            case 1: return br_cluster_kernel<BR_LOGN, 1, false, 4>;
+            case 2: return br_cluster_kernel<BR_LOGN, 2, false, 4>;
+            case 3: return br_cluster_kernel<BR_LOGN, 3, false, 4>;
+            default: return nullptr;
+        }
+    }
+#endif
+    return nullptr;
 }
 #endif
 

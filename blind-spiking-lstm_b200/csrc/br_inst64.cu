@@ -3,7 +3,7 @@
 // Shapes: the one-CTA layout with extra threads, the quarter-root-table-in-
 // global layout, and the plain layout; l_bs 1 .. 3; and the cluster-pair
 // kernel of small batches (br_split.cuh).
-#include "br_quad.cuh"
+#include "br_cluster.cuh"
 #include "br_split.cuh"
 #include "br_tm.cuh"
 #include "tfhe_dispatch.h"
@@ -47,13 +47,26 @@ BrKernel TFHE_CAT(br_split64_logn_, BR_LOGN)(int L) {
 }
 
 #if BR_LOGN == 10 || BR_LOGN == 11
-BrKernel TFHE_CAT(br_quad64_logn, BR_LOGN)(int L) {
-    switch (L) {
-        case 1: return br_quad_kernel<BR_LOGN, 1, true>;
-        case 2: return br_quad_kernel<BR_LOGN, 2, true>;
-        case 3: return br_quad_kernel<BR_LOGN, 3, true>;
-        default: return nullptr;
+BrKernel TFHE_CAT(br_cluster64_logn, BR_LOGN)(int L, int S) {
+    if (S == 2) {
+        switch (L) {
+            case 1: return br_cluster_kernel<BR_LOGN, 1, true, 2>;
+            case 2: return br_cluster_kernel<BR_LOGN, 2, true, 2>;
+            case 3: return br_cluster_kernel<BR_LOGN, 3, true, 2>;
+            default: return nullptr;
+        }
     }
+#if BR_LOGN == 11
+    if (S == 4) {
+        switch (L) {
+            case 1: return br_cluster_kernel<BR_LOGN, 1, true, 4>;
+            case 2: return br_cluster_kernel<BR_LOGN, 2, true, 4>;
+            case 3: return br_cluster_kernel<BR_LOGN, 3, true, 4>;
+            default: return nullptr;
+        }
+    }
+#endif
+    return nullptr;
 }
 #endif
 

@@ -424,12 +424,14 @@ static int launch_split(const BrArgs& args, int N, int L, cudaStream_t stream, c
                           stream, tune, "blind rotation launch (cluster pair)");
 }
 
-static int launch_quad(const BrArgs& args, int N, int L, cudaStream_t stream, const tfhe_tuning* tune) {
+// one ciphertext per cluster of 2 S CTAs (br_cluster.cuh)
+static int launch_cluster_s(const BrArgs& args, int N, int L, int S, cudaStream_t stream, const tfhe_tuning* tune) {
     const bool t64 = args.lwe_a64 != nullptr;
-    BrKernel kern = br_quad_kernel_for(ilog2(N), L, t64);
+    BrKernel kern = br_cluster_kernel_for(ilog2(N), L, t64, S);
     if (!kern) return fail(TFHE_ERR_INVALID_ARGUMENT, "unsupported degree / levels");
-    return launch_cluster(kern, BR_QUAD_THREADS, br_quad_smem(N, L, args.G, args.M, br_table_bytes(N)), 4, args, N,
-                          stream, tune, "blind rotation launch (cluster of four)");
+    return launch_cluster(kern, BR_CLUSTER_THREADS, br_cluster_smem(N, L, args.G, args.M, br_table_bytes(N), S),
+                          2 * S, args, N, stream, tune,
+                          S == 4 ? "blind rotation launch (cluster of eight)" : "blind rotation launch (cluster of four)");
 }
 
 // clusters of `csize` CTAs of this kernel that can be resident at once (a
@@ -472,10 +474,11 @@ static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
                              br_split_smem(N, L, G, M, br_table_bytes(N)), 2);
 }
 
-// One ciphertext per cluster of four CTAs (br_quad.cuh) at N = 1024 and 2048
-// for batches that fit one wave of such clusters: half the pair's per-SM key
-// traffic in the pointwise stage.  TFHE_B200_QUAD=0 turns it off (the pair
-// then takes those batches).
+// One ciphertext per cluster of 2 S CTAs (br_cluster.cuh): eight CTAs (S = 4)
+// at N = 2048, four (S = 2) at N = 1024 and 2048, for batches that fit one
+// wave of such clusters; each SM then pulls 1 / (2 S) of a group's key in the
+// pointwise stage.  TFHE_B200_QUAD=0 turns both off (the pair then takes those
+// batches), TFHE_B200_OCTET=0 only the clusters of eight.
 static bool quad_enabled() {
     static const bool on = [] {
         const char* env = getenv("TFHE_B200_QUAD");
@@ -484,15 +487,32 @@ static bool quad_enabled() {
     return on;
 }
 
-static bool quad_applies(int N, int L, int G, int M, long long B, bool reflayout, int kr, const tfhe_tuning* tune,
-                         bool t64) {
+static bool octet_enabled() {
+    static const bool on = [] {
+        const char* env = getenv("TFHE_B200_OCTET");
+        return !(env && env[0] == '0');
+    }();
+    return on;
+}
+
+// CTAs per polynomial (S = 4 or 2) of the widest cluster form that takes this
+// batch, 0 for none
+static int cluster_form(int N, int L, int G, int M, long long B, bool reflayout, int kr, const tfhe_tuning* tune,
+                        bool t64) {
     const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
-    if (kr != 0 || reflayout || requested || L > 3 || M > BR_QUAD_MAX_M || M < 2 || !quad_enabled() ||
-        !split_enabled() || B < 1 || 4 * B > sm_count())
-        return false;
-    BrKernel kern = br_quad_kernel_for(ilog2(N), L, t64);
-    if (!kern) return false;
-    return B <= resident_clusters(kern, BR_QUAD_THREADS, br_quad_smem(N, L, G, M, br_table_bytes(N)), 4);
+    if (kr != 0 || reflayout || requested || L > 3 || M > BR_CLUSTER_MAX_M || M < 2 || !quad_enabled() ||
+        !split_enabled() || B < 1)
+        return 0;
+    for (int S : {4, 2}) {
+        if (S == 4 && !octet_enabled()) continue;
+        if (2 * S * B > sm_count()) continue;
+        BrKernel kern = br_cluster_kernel_for(ilog2(N), L, t64, S);
+        if (!kern) continue;
+        if (B <= resident_clusters(kern, BR_CLUSTER_THREADS, br_cluster_smem(N, L, G, M, br_table_bytes(N), S),
+                                   2 * S))
+            return S;
+    }
+    return 0;
 }
 
 static bool split_applies(int N, int L, int G, int M, long long B, bool reflayout, int kr,
@@ -563,8 +583,8 @@ static int launch_br(BrArgs args, int N, int L, bool reflayout, int kr, cudaStre
                      int* status = nullptr, const tfhe_tuning* tune = nullptr) {
     const int logn = ilog2(N);
     const bool requested = (tune && tune->ciphertexts_per_cta > 0) || k_override() > 0;
-    if (quad_applies(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
-        return launch_quad(args, N, L, stream, tune);
+    if (const int S = cluster_form(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
+        return launch_cluster_s(args, N, L, S, stream, tune);
     if (split_applies(N, L, args.G, args.M, args.B, reflayout, kr, tune, args.lwe_a64 != nullptr))
         return launch_split(args, N, L, stream, tune);
     if (!reflayout && kr == 0 && N == 2048 && L <= 2 &&
@@ -1443,7 +1463,8 @@ int32_t tfhe_keys_cluster_size(const tfhe_keys* keys, int64_t batch) {
     if (!keys) return 0;
     const tfhe_params& p = keys->p;
     const bool t64 = p.log2_q == 64;
-    if (quad_applies(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, t64)) return 4;
+    if (const int S = cluster_form(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, t64))
+        return 2 * S;
     return split_applies(p.N, p.l_bs, keys->G, keys->M, batch, false, keys->ring_kr, &keys->tune, t64) ? 2 : 1;
 }
 

@@ -2,7 +2,7 @@
 // the FP64 blind-rotation kernels and the key-FFT kernel of its degree.
 #pragma once
 
-#include "br_quad.cuh"
+#include "br_cluster.cuh"
 #include "br_split.cuh"
 #include "br_tm.cuh"
 
@@ -65,14 +65,15 @@ inline BrKernel br_split_kernel_for(int logn, int L, bool t64) {
     }
 }
 
-// the cluster-of-four kernels of small batches, N = 1024 and 2048
-BrKernel br_quad32_logn10(int L);
-BrKernel br_quad32_logn11(int L);
-BrKernel br_quad64_logn10(int L);
-BrKernel br_quad64_logn11(int L);
-inline BrKernel br_quad_kernel_for(int logn, int L, bool t64) {
-    if (logn == 10) return t64 ? br_quad64_logn10(L) : br_quad32_logn10(L);
-    if (logn == 11) return t64 ? br_quad64_logn11(L) : br_quad32_logn11(L);
+// the kernels of one ciphertext per cluster of 2 S CTAs for small batches:
+// S = 2 (four CTAs) at N = 1024 and 2048, S = 4 (eight CTAs) at N = 2048
+BrKernel br_cluster32_logn10(int L, int S);
+BrKernel br_cluster32_logn11(int L, int S);
+BrKernel br_cluster64_logn10(int L, int S);
+BrKernel br_cluster64_logn11(int L, int S);
+inline BrKernel br_cluster_kernel_for(int logn, int L, bool t64, int S) {
+    if (logn == 10) return t64 ? br_cluster64_logn10(L, S) : br_cluster32_logn10(L, S);
+    if (logn == 11) return t64 ? br_cluster64_logn11(L, S) : br_cluster32_logn11(L, S);
     return nullptr;
 }
 

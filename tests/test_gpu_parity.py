@@ -518,21 +518,24 @@ def test_keyswitch_unaligned_input_uses_cuda_cores():
     assert np.array_equal(host_u32(ga), u32(ra)) and np.array_equal(host_u32(gb), u32(rb.reshape(-1)))
 
 
-def quad_form(name):
-    """whether small batches of this set run on clusters of four CTAs"""
+def small_batch_cluster(name):
+    """CTAs per ciphertext of this set's smallest batches: eight at N = 2048
+    and four at N = 1024 (collapse <= 3), else two"""
     p = PARAMS[name]
-    return p["N"] in (1024, 2048) and p["l_bs"] <= 3 and 2 ** p["collapse"] <= 8
+    if p["l_bs"] <= 3 and 2 ** p["collapse"] <= 8:
+        return {2048: 8, 1024: 4}.get(p["N"], 2)
+    return 2
 
 
 @pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2", "c1_N128", "c4_N4096", "c1_N1024_l1",
                                   "c3_N2048_l3"])
 def test_cluster_kernels_match_one_cta_kernel(name):
-    """Small batches run one ciphertext on a cluster of four CTAs (N = 1024
-    and 2048, collapse <= 3: each CTA owns one ACC polynomial and half of the
-    spectrum) or of two (each owns one ACC polynomial); the outputs are
-    bit-identical to the one-CTA kernel's (requested shape K = 1), at every
-    parameter set, for the extraction (n_lut 1 and 4) and for the rotated
-    accumulator."""
+    """Small batches run one ciphertext on a cluster of eight CTAs (N = 2048)
+    or four (N = 1024 and 2048; collapse <= 3: each CTA owns one ACC
+    polynomial and a quarter or half of the spectrum) or of two (each owns one
+    ACC polynomial); the outputs are bit-identical to the one-CTA kernel's
+    (requested shape K = 1), at every parameter set, for the extraction
+    (n_lut 1 and 4) and for the rotated accumulator."""
     p = PARAMS[name]
     N = p["N"]
     eng = engine(name)
@@ -545,7 +548,7 @@ def test_cluster_kernels_match_one_cta_kernel(name):
         eng.set_tuning()
         cs = eng.cluster_size(batch)
         if batch <= 5:
-            assert cs == (4 if quad_form(name) else 2), (batch, cs)
+            assert cs == small_batch_cluster(name), (batch, cs)
         elif batch == sms // 2:
             assert cs == 2, (batch, cs)
         else:

@@ -152,9 +152,10 @@ def test_native_and_reference_layout_chains_agree64():
 
 
 def test_cluster_kernels_match_one_cta_kernel64():
-    """Small batches on clusters of four CTAs (up to a quarter of the SM
-    count) and of two give the one-CTA kernel's outputs bit for bit on the
-    64-bit torus (reference parameters, n_lut 1 and 4)."""
+    """Small batches on clusters of eight CTAs (up to an eighth of the SM
+    count), of four (up to a quarter) and of two give the one-CTA kernel's
+    outputs bit for bit on the 64-bit torus (reference parameters, n_lut 1
+    and 4)."""
     p = C64.REF64
     ck, dk, ok = keys_for(p)
     rng = np.random.default_rng(45)
@@ -164,7 +165,7 @@ def test_cluster_kernels_match_one_cta_kernel64():
         dk.set_tuning()
         cs = dk.cluster_size(B)
         if B <= 6:
-            assert cs == 4, (B, cs)
+            assert cs == 8, (B, cs)
         elif B == sms // 2:
             assert cs == 2, (B, cs)
         else:
