@@ -149,8 +149,9 @@ class Keys:
         return k.value, nt.value, sm.value
 
     def cluster_size(self, batch: int) -> int:
-        """CTAs per ciphertext of a batch's blind rotation: 2 where one
-        ciphertext runs on a cluster pair (small batches), else 1."""
+        """CTAs per ciphertext of a batch's blind rotation: 8, 4 or 2 where
+        one ciphertext runs on a cluster of that many CTAs (small batches),
+        else 1."""
         return int(_lib.load().tfhe_keys_cluster_size(self.handle, int(batch)))
 
     def device_bytes(self) -> int:

@@ -92,7 +92,8 @@ class Keys64:
         self.ks_tensor_cores = int(ks_tensor_cores)
 
     def cluster_size(self, batch: int) -> int:
-        """CTAs per ciphertext of a batch's blind rotation (2: cluster pair)."""
+        """CTAs per ciphertext of a batch's blind rotation (8, 4 or 2: one
+        ciphertext per cluster of that many CTAs; 1: several per CTA)."""
         return int(_lib.load().tfhe_keys_cluster_size(self.handle, int(batch)))
 
     def close(self):
