@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--hidden", type=int, default=128)
     ap.add_argument("--layers", type=int, default=1)
     ap.add_argument("--graph", action="store_true", help="--lstm: replay each timestep from a CUDA graph")
+    ap.add_argument("--direct", action="store_true",
+                    help="--serve: launch every tick's kernels directly (no CUDA-graph replay of ticks)")
     ap.add_argument("--torus", type=int, choices=[32, 64], default=32,
                     help="--lstm / --serve: the 2^32 torus (config-1 bootstrapping) or the reference's own 2^64")
     ap.add_argument("--serve", action="store_true",
@@ -515,7 +517,7 @@ def run_serve(args):
            else SM.SpikeModelConfig(hidden=hidden, layers=layers))
     model = SM.build_model(cfg, args.seed)
     dm = SM.to_device(model, dev)
-    sm = DeviceStepModel(dm)
+    sm = DeviceStepModel(dm, graphs=False if getattr(args, "direct", False) else None)
     rng = np.random.default_rng(args.seed + 9)
     t_max = 64
     free, _ = torch.cuda.mem_get_info()
@@ -571,7 +573,8 @@ def run_serve(args):
             "data": "synthetic: Poisson arrivals, U[8,64] Zipf(1.1) tokens, random int weights",
             "config": {"workload": "Spike-LSTM serving", "rate_req_per_s": args.rate, "requests": len(done),
                        "layers": cfg.layers, "hidden": cfg.hidden, "emb_dim": cfg.emb_dim, "n_lut": cfg.n_lut,
-                       "slots": slots, "pbs": cfg.pbs.name, "torus": f"q = 2^{cfg.torus_bits}"},
+                       "slots": slots, "pbs": cfg.pbs.name, "torus": f"q = 2^{cfg.torus_bits}",
+                       "ticks": "direct launches" if sm.graphs is None else "CUDA-graph replay"},
             "latency": {k2: (round(v, 3) if isinstance(v, float) else v) for k2, v in lat.items()},
             "tokens_per_s": round(tokens / span, 2), "ticks": srv.ticks,
             "mean_batch": round(float(np.mean(srv.batch_sizes)), 2), "max_batch": int(max(srv.batch_sizes)),

@@ -67,15 +67,49 @@ class StepModel:
         raise NotImplementedError
 
 
+class _TickGraph:
+    """step_merged of one combination of per-layer request counts, captured
+    in a CUDA graph on fixed input buffers: a tick then costs a few copies
+    and one graph launch instead of its several dozen kernel launches and
+    their host work.  The outputs are the graph's, valid until its next
+    replay."""
+
+    def __init__(self, model, xs, states):
+        self.xs = [x.clone() for x in xs]
+        self.states = [st.clone() for st in states]
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.out = model._step_layers(self.xs, self.states)
+
+    def run(self, xs, states):
+        for dst, src in zip(self.xs, xs):
+            dst.copy_(src)
+        for dst, src in zip(self.states, states):
+            dst.copy_(src)
+        self.graph.replay()
+        return self.out
+
+
 class DeviceStepModel(StepModel):
     """The engine's encrypted layers and head (spike_model.DeviceModel); the
-    layers' bootstraps of one tick run as one launch per phase."""
+    layers' bootstraps of one tick run as one launch per phase.  With
+    graphs (the default on the 2^32 torus) a tick whose per-layer request
+    counts were seen before replays a CUDA graph of the step: the first
+    tick of a combination runs directly (its launches fill the engine's
+    per-shape caches), the second captures the graph, later ones replay it.
+    Results are identical either way (the same kernels on the same data).
+    The 2^64 torus runs direct launches unless graphs=True is asked for."""
 
-    def __init__(self, dm):
+    def __init__(self, dm, graphs=None):
         self.dm = dm
         self.N = dm.keys.galois.N
         self.n_layers = len(dm.layers)
         self.dtype = torch.int64 if dm.keys.torus_bits == 64 else torch.int32
+        if graphs is None:
+            graphs = dm.keys.torus_bits == 32
+        self.graphs = {} if graphs else None
+        self._seen = set()
 
     def state_shape(self):
         return (2, 2, self.N)
@@ -85,6 +119,18 @@ class DeviceStepModel(StepModel):
         return rlwe_rotate_add(prev_states[:, 0].contiguous(), -self.dm.layers[layer - 1].input_dim)
 
     def step_layers(self, xs, states):
+        if self.graphs is None:
+            return self._step_layers(xs, states)
+        key = tuple(int(x.shape[0]) for x in xs)
+        g = self.graphs.get(key)
+        if g is None:
+            if key not in self._seen:
+                self._seen.add(key)
+                return self._step_layers(xs, states)
+            g = self.graphs[key] = _TickGraph(self, xs, states)
+        return g.run(xs, states)
+
+    def _step_layers(self, xs, states):
         from .lstm import step_merged
         items, which = [], []
         for li, (x, st) in enumerate(zip(xs, states)):
