@@ -500,9 +500,10 @@ def run_serve(args):
     encrypted sequence of U[8, 64] Zipf(1.1) tokens; 2-layer Spike-LSTM with
     hidden 256 (layers and hidden from the flags when given), per-request
     encrypted state kept on the GPU, continuous batching (every live
-    request's current timestep in one batched step).  Reports p50/p99
-    latency and sequences/s, next to the same requests served one at a time
-    (one slot: no batching across requests)."""
+    request's current timestep in one batched step; ticks replayed from CUDA
+    graphs per combination of request counts, or launched directly with
+    --direct).  Reports p50/p99 latency and sequences/s, next to the same
+    requests served one at a time (one slot: no batching across requests)."""
     import numpy as np
     import torch
     from tfhe_b200 import spike_model as SM
