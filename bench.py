@@ -535,7 +535,9 @@ def run_serve(args):
             out.append(Request(i, xs, arrival=float(arr[i])))
         return out
 
-    # warm-up: two short requests through a server
+    # warm-up: the ticks of up to four requests per layer captured as graphs
+    # ahead of the timed run, then two short requests through a server
+    sm.warm_graphs(4)
     warm = SpikeLstmServer(sm, 2, t_max, dev)
     for r in make_requests(2, 100.0):
         r.xs = r.xs[:2].contiguous()

@@ -17,10 +17,10 @@
 //     after a second cluster barrier the S CTAs of polynomial r each run the
 //     last superstage over all parts (8/S of its 8 points per part), so each
 //     holds the whole next ACC polynomial r for its next prologue.
-// Where a part holds half as many positions as the CTA has threads, two
-// adjacent lanes share a position, lane 0 contracting the first M/2 patterns
-// and lane 1 the others, and lane 1 continues lane 0's sum after one shuffle,
-// so the sum over patterns keeps its order.  Every value is computed by the
+// Where a part holds fewer positions than the CTA has threads, TPS = 2 or 4
+// adjacent lanes share a position, lane u contracting the u-th M/TPS
+// patterns, and each lane continues the sum of the lanes before it after a
+// shuffle, so the sum over patterns keeps its order.  Every value is computed by the
 // same operations in the same order as br_fp64_kernel (digits, FFT stages,
 // the key contraction in digit order per pattern, the twist products in
 // pattern order, the rounding), so the outputs are bit-identical to it.
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(BR_CLUSTER_THREADS, 1) br_cluster_kernel(const
     constexpr int TPS = BR_CLUSTER_THREADS / PART;       // lanes per position in the pointwise stage
     using PL = Plan<LOGH>;
     static_assert(S == 2 || S == 4, "clusters of four or eight CTAs");
-    static_assert(TPS == 1 || TPS == 2, "one or two lanes per position");
+    static_assert(TPS == 1 || TPS == 2 || TPS == 4, "one, two or four lanes per position");
     static_assert(Q8 * PPP == PART, "the last superstage reads 8/S points of each part");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -308,10 +308,11 @@ __global__ void __launch_bounds__(BR_CLUSTER_THREADS, 1) br_cluster_kernel(const
                     outp[swz(p)] = o;
                 } else {
                     // lane u of the position contracts patterns
-                    // [u M/2, (u+1) M/2); lane 0 also applies its twists, lane 1
-                    // keeps its sums until lane 0's total arrives
-                    const int u = tid & 1;
-                    const int mlen = M >> 1;
+                    // [u M/TPS, (u+1) M/TPS) (M a multiple of TPS); lane 0
+                    // also applies its twists, the other lanes keep their
+                    // sums until the total of the lanes before them arrives
+                    const int u = tid % TPS;
+                    const int mlen = M / TPS;
                     const int mbeg = u * mlen;
                     double2 tt[BR_CLUSTER_MAX_M / 2];
 #pragma unroll
@@ -334,19 +335,23 @@ __global__ void __launch_bounds__(BR_CLUSTER_THREADS, 1) br_cluster_kernel(const
                             }
                         }
                     }
-                    double2 prev;
-                    prev.x = __shfl_up_sync(0xffffffffu, o.x, 1);
-                    prev.y = __shfl_up_sync(0xffffffffu, o.y, 1);
-                    if (u == 1) {
-                        o = prev;
 #pragma unroll
-                        for (int i = 0; i < BR_CLUSTER_MAX_M / 2; ++i)
-                            if (i < mlen) {
-                                const double2 w = root2n<LOGN, true>(qt_s, rot[mbeg + i] * e);
-                                c_mac(o, w, tt[i]);
-                            }
-                        outp[swz(p)] = o;
+                    for (int lane = 1; lane < TPS; ++lane) {
+                        // lane `lane` continues the sum of lanes 0 .. lane - 1
+                        double2 prev;
+                        prev.x = __shfl_up_sync(0xffffffffu, o.x, 1);
+                        prev.y = __shfl_up_sync(0xffffffffu, o.y, 1);
+                        if (u == lane) {
+                            o = prev;
+#pragma unroll
+                            for (int i = 0; i < BR_CLUSTER_MAX_M / 2; ++i)
+                                if (i < mlen) {
+                                    const double2 w = root2n<LOGN, true>(qt_s, rot[mbeg + i] * e);
+                                    c_mac(o, w, tt[i]);
+                                }
+                        }
                     }
+                    if (u == TPS - 1) outp[swz(p)] = o;
                 }
             }
             __syncthreads();

@@ -77,7 +77,6 @@ BrKernel TFHE_CAT(br_cluster32_logn, BR_LOGN)(int L, int S) {
             default: return nullptr;
         }
     }
-#if BR_LOGN == 11
     if (S == 4) {
         switch (L) {
             case 1: return br_cluster_kernel<BR_LOGN, 1, false, 4>;
@@ -86,7 +85,6 @@ BrKernel TFHE_CAT(br_cluster32_logn, BR_LOGN)(int L, int S) {
             default: return nullptr;
         }
     }
-#endif
     return nullptr;
 }
 #endif

@@ -56,7 +56,6 @@ BrKernel TFHE_CAT(br_cluster64_logn, BR_LOGN)(int L, int S) {
             default: return nullptr;
         }
     }
-#if BR_LOGN == 11
     if (S == 4) {
         switch (L) {
             case 1: return br_cluster_kernel<BR_LOGN, 1, true, 4>;
@@ -65,7 +64,6 @@ BrKernel TFHE_CAT(br_cluster64_logn, BR_LOGN)(int L, int S) {
             default: return nullptr;
         }
     }
-#endif
     return nullptr;
 }
 #endif

@@ -475,8 +475,8 @@ static long long split_resident_clusters(int N, int L, int G, int M, bool t64) {
 }
 
 // One ciphertext per cluster of 2 S CTAs (br_cluster.cuh): eight CTAs (S = 4)
-// at N = 2048, four (S = 2) at N = 1024 and 2048, for batches that fit one
-// wave of such clusters; each SM then pulls 1 / (2 S) of a group's key in the
+// or four (S = 2) at N = 1024 and 2048, for batches that fit one wave of
+// such clusters (eight at N = 1024 needs at least four patterns); each SM then pulls 1 / (2 S) of a group's key in the
 // pointwise stage.  TFHE_B200_QUAD=0 turns both off (the pair then takes those
 // batches), TFHE_B200_OCTET=0 only the clusters of eight.
 static bool quad_enabled() {
@@ -506,6 +506,9 @@ static int cluster_form(int N, int L, int G, int M, long long B, bool reflayout,
     for (int S : {4, 2}) {
         if (S == 4 && !octet_enabled()) continue;
         if (2 * S * B > sm_count()) continue;
+        // lanes per position in the pointwise stage: each takes M / lanes patterns
+        const int lanes = BR_CLUSTER_THREADS / (N / 2 / S);
+        if (lanes > 1 && M % lanes != 0) continue;
         BrKernel kern = br_cluster_kernel_for(ilog2(N), L, t64, S);
         if (!kern) continue;
         if (B <= resident_clusters(kern, BR_CLUSTER_THREADS, br_cluster_smem(N, L, G, M, br_table_bytes(N), S),

@@ -66,7 +66,7 @@ inline BrKernel br_split_kernel_for(int logn, int L, bool t64) {
 }
 
 // the kernels of one ciphertext per cluster of 2 S CTAs for small batches:
-// S = 2 (four CTAs) at N = 1024 and 2048, S = 4 (eight CTAs) at N = 2048
+// S = 2 (four CTAs) and S = 4 (eight CTAs) at N = 1024 and 2048
 BrKernel br_cluster32_logn10(int L, int S);
 BrKernel br_cluster32_logn11(int L, int S);
 BrKernel br_cluster64_logn10(int L, int S);

@@ -130,6 +130,24 @@ class DeviceStepModel(StepModel):
             g = self.graphs[key] = _TickGraph(self, xs, states)
         return g.run(xs, states)
 
+    def warm_graphs(self, max_count: int):
+        """Run and capture ahead of time the tick of every combination of
+        per-layer request counts up to max_count (on zero ciphertexts), so a
+        serving run meets no capture on its latency path for them."""
+        import itertools
+        if self.graphs is None:
+            return
+        dev = self.dm.layers[0].device
+        for key in itertools.product(range(max_count + 1), repeat=self.n_layers):
+            if not any(key) or key in self.graphs:
+                continue
+            xs = [torch.zeros((c, 2, self.N), dtype=self.dtype, device=dev) for c in key]
+            states = [torch.zeros((c,) + tuple(self.state_shape()), dtype=self.dtype, device=dev) for c in key]
+            self._seen.add(key)
+            self._step_layers(xs, states)
+            self.graphs[key] = _TickGraph(self, xs, states)
+        torch.cuda.synchronize()
+
     def _step_layers(self, xs, states):
         from .lstm import step_merged
         items, which = [], []

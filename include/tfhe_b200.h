@@ -123,9 +123,10 @@ int tfhe_keys_launch_shape(const tfhe_keys* keys, int64_t batch, int32_t* cipher
                            int32_t* threads, int64_t* shared_bytes);
 
 /* CTAs per ciphertext a batch's blind rotation takes: 8 where one
- * ciphertext runs on a cluster of eight CTAs (N = 2048, collapse <= 3,
- * batches of at most an eighth of the SM count; TFHE_B200_OCTET=0 turns it
- * off), 4 on a cluster of four (N = 1024 or 2048, at most a quarter;
+ * ciphertext runs on a cluster of eight CTAs (N = 1024 or 2048, collapse
+ * <= 3, at N = 1024 collapse >= 2; batches of at most an eighth of the SM
+ * count; TFHE_B200_OCTET=0 turns it off), 4 on a cluster of four (N = 1024
+ * or 2048, at most a quarter;
  * TFHE_B200_QUAD=0 turns both off), 2 on a cluster of two (at most half the
  * SM count), else 1 (automatic shapes only; TFHE_B200_SPLIT=0 turns every
  * cluster form off); 0 for NULL keys.  Speed only: every form gives

@@ -520,20 +520,21 @@ def test_keyswitch_unaligned_input_uses_cuda_cores():
 
 def small_batch_cluster(name):
     """CTAs per ciphertext of this set's smallest batches: eight at N = 2048
-    and four at N = 1024 (collapse <= 3), else two"""
+    and at N = 1024 with four or eight patterns, four at N = 1024 with two
+    (collapse <= 3), else two"""
     p = PARAMS[name]
-    if p["l_bs"] <= 3 and 2 ** p["collapse"] <= 8:
-        return {2048: 8, 1024: 4}.get(p["N"], 2)
+    if p["l_bs"] <= 3 and 2 ** p["collapse"] <= 8 and p["N"] in (1024, 2048):
+        return 4 if (p["N"] == 1024 and p["collapse"] == 1) else 8
     return 2
 
 
 @pytest.mark.parametrize("name", ["tiny_c3", "tiny_c2", "cfg1", "cfg2", "c1_N128", "c4_N4096", "c1_N1024_l1",
                                   "c3_N2048_l3"])
 def test_cluster_kernels_match_one_cta_kernel(name):
-    """Small batches run one ciphertext on a cluster of eight CTAs (N = 2048)
-    or four (N = 1024 and 2048; collapse <= 3: each CTA owns one ACC
-    polynomial and a quarter or half of the spectrum) or of two (each owns one
-    ACC polynomial); the outputs are bit-identical to the one-CTA kernel's
+    """Small batches run one ciphertext on a cluster of eight or four CTAs
+    (N = 1024 and 2048, collapse <= 3: each CTA owns one ACC polynomial and a
+    quarter or half of the spectrum) or of two (each owns one ACC
+    polynomial); the outputs are bit-identical to the one-CTA kernel's
     (requested shape K = 1), at every parameter set, for the extraction
     (n_lut 1 and 4) and for the rotated accumulator."""
     p = PARAMS[name]

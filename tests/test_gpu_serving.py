@@ -43,3 +43,11 @@ def test_results_alone_equal_results_in_the_mix():
         assert torch.equal(a[0].cpu(), mixed[i][0]) and torch.equal(b[0].cpu(), mixed[i][1]), i
     # repeated request-count combinations were replayed from captured graphs
     assert len(sm.graphs) > 0
+    # graphs captured ahead of time give the same logits as well
+    sm2 = DeviceStepModel(dm)
+    sm2.warm_graphs(2)
+    assert (1, 0) in sm2.graphs and (2, 2) in sm2.graphs
+    sm = sm2
+    again = serve(range(len(reqs)), 3)
+    for i in range(len(reqs)):
+        assert torch.equal(again[i][0], mixed[i][0]) and torch.equal(again[i][1], mixed[i][1]), i
