@@ -58,8 +58,8 @@ def parse():
                     help="one encrypted Spike-LSTM layer + head: sequences/s (one GPU)")
     ap.add_argument("--seq-len", type=int, default=32)
     ap.add_argument("--seqs", type=int, default=16)
-    ap.add_argument("--hidden", type=int, default=128)
-    ap.add_argument("--layers", type=int, default=1)
+    ap.add_argument("--hidden", type=int, default=None, help="hidden units (default 128 with --lstm, 256 with --serve)")
+    ap.add_argument("--layers", type=int, default=None, help="layers (default 1 with --lstm, 2 with --serve)")
     ap.add_argument("--graph", action="store_true", help="--lstm: replay each timestep from a CUDA graph")
     ap.add_argument("--direct", action="store_true",
                     help="--serve: launch every tick's kernels directly (no CUDA-graph replay of ticks)")
@@ -314,7 +314,7 @@ def serving_summary(args):
     batching), reduced to its latency percentiles and throughput."""
     import argparse
     sargs = argparse.Namespace(**vars(args))
-    sargs.rate, sargs.requests, sargs.torus, sargs.hidden, sargs.layers = 2.0, 24, 32, 128, 1
+    sargs.rate, sargs.requests, sargs.torus, sargs.hidden, sargs.layers = 2.0, 24, 32, None, None
     sargs.warmup = 1
     out = run_serve(sargs)
     return {"workload": "Spike-LSTM serving (config 5): Poisson 2 req/s, 24 requests of U[8,64] tokens, "
@@ -419,8 +419,10 @@ def run_lstm(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
-    cfg = (SM.config_q64(hidden=args.hidden, layers=args.layers) if args.torus == 64
-           else SM.SpikeModelConfig(hidden=args.hidden, layers=args.layers))
+    hidden = args.hidden or 128
+    layers = args.layers or 1
+    cfg = (SM.config_q64(hidden=hidden, layers=layers) if args.torus == 64
+           else SM.SpikeModelConfig(hidden=hidden, layers=layers))
     model = SM.build_model(cfg, args.seed)
     dm = SM.to_device(model, dev)
     rng = np.random.default_rng(args.seed + 5)
@@ -512,8 +514,8 @@ def run_serve(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
-    hidden = args.hidden if args.hidden != 128 else 256
-    layers = args.layers if args.layers != 1 else 2
+    hidden = args.hidden or 256
+    layers = args.layers or 2
     cfg = (SM.config_q64(hidden=hidden, layers=layers) if args.torus == 64
            else SM.SpikeModelConfig(hidden=hidden, layers=layers))
     model = SM.build_model(cfg, args.seed)
