@@ -99,9 +99,12 @@ class DeviceStepModel(StepModel):
     tick of a combination runs directly (its launches fill the engine's
     per-shape caches), the second captures the graph, later ones replay it.
     Results are identical either way (the same kernels on the same data).
-    The 2^64 torus runs direct launches unless graphs=True is asked for."""
+    The 2^64 torus runs direct launches unless graphs=True is asked for.
+    Only ticks of at most graph_max requests per layer are graphed (each
+    graph keeps its own working memory; larger ticks have launch work to
+    spare anyway), so the cache stays at (graph_max + 1)^layers graphs."""
 
-    def __init__(self, dm, graphs=None):
+    def __init__(self, dm, graphs=None, graph_max: int = 8):
         self.dm = dm
         self.N = dm.keys.galois.N
         self.n_layers = len(dm.layers)
@@ -109,6 +112,7 @@ class DeviceStepModel(StepModel):
         if graphs is None:
             graphs = dm.keys.torus_bits == 32
         self.graphs = {} if graphs else None
+        self.graph_max = graph_max
         self._seen = set()
 
     def state_shape(self):
@@ -122,6 +126,8 @@ class DeviceStepModel(StepModel):
         if self.graphs is None:
             return self._step_layers(xs, states)
         key = tuple(int(x.shape[0]) for x in xs)
+        if max(key) > self.graph_max:
+            return self._step_layers(xs, states)
         g = self.graphs.get(key)
         if g is None:
             if key not in self._seen:
@@ -138,7 +144,7 @@ class DeviceStepModel(StepModel):
         if self.graphs is None:
             return
         dev = self.dm.layers[0].device
-        for key in itertools.product(range(max_count + 1), repeat=self.n_layers):
+        for key in itertools.product(range(min(max_count, self.graph_max) + 1), repeat=self.n_layers):
             if not any(key) or key in self.graphs:
                 continue
             xs = [torch.zeros((c, 2, self.N), dtype=self.dtype, device=dev) for c in key]
